@@ -1,0 +1,203 @@
+/*
+ * trajsparsenufft.h — C ABI of the B200 (sm_100a) fixed-trajectory NUFFT CG-SENSE library.
+ *
+ * The reference exposes this path as files + argv + a 7-function FFT C ABI:
+ *   - pack directories written by src/export_gpu_case.py:171-321 and
+ *     src/export_torchkbnufft_gpu_case.py:387-489 (packed_header_v2),
+ *   - loaded by load_direction()     experiments/production/src/nufft_integrated_bench.cu:135-226,
+ *   - runtime inputs (measurement.c64.bin [C][M], sensitivity_maps.c64.bin [C][N][N],
+ *     scaling.f32.bin [N][N], density.f32.bin [M])
+ *                                      experiments/data_prep/export_real_runtime_inputs.py:92-113,
+ *   - FFT endpoints                    experiments/production/src/nufft_custom_fft_f30_api.h:6-34,
+ *   - the CG driver main()             experiments/production/src/nufft_fp16x2_cg_bench.cu:279-518.
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions (kept from the reference):
+ *   - complex data are interleaved float pairs (float2 / complex64);
+ *   - coil-major layouts: samples [C][M], coil images / maps [C][N][N], image [N][N];
+ *   - grid cell index = q0*G + q1 in pack files (nufft_custom_fft_forward_bench.cu:699-701);
+ *   - the image sits at [0,N) of the G x G grid and the phase is carried by the
+ *     complex coefficients;
+ *   - trajectories are cycles/pixel in [-0.5, 0.5), axis 0 pairs with image axis 0.
+ * Every call returns a tsn_status; nothing calls exit().  Device pointers are
+ * caller-owned; the plan owns packs and workspaces.  A plan is not thread-safe,
+ * separate plans may be used concurrently from separate threads/streams.
+ */
+#ifndef TRAJSPARSENUFFT_H_
+#define TRAJSPARSENUFFT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same underlying type as cudaStream_t; NULL is the legacy default stream. */
+typedef struct CUstream_st* tsn_stream_t;
+
+typedef enum tsn_status {
+  TSN_OK = 0,
+  TSN_ERR_IO = 1,          /* file missing, short or unwritable     (reference: exit(1)) */
+  TSN_ERR_FORMAT = 2,      /* bad magic/version/header, real/imag mismatch (exit(2))  */
+  TSN_ERR_SHAPE = 3,       /* sizes inconsistent with the plan                         */
+  TSN_ERR_NONFINITE = 4,   /* non-finite input or CG state (reference exit(3))        */
+  TSN_ERR_CURVATURE = 5,   /* CG denominator <= 0 (positive_curvature flag = 0)        */
+  TSN_ERR_TIMEOUT = 6,     /* a bounded device wait gave up                            */
+  TSN_ERR_CUDA = 7,        /* CUDA runtime error                                       */
+  TSN_ERR_ARG = 8,         /* invalid argument / NULL where required                   */
+  TSN_ERR_UNSUPPORTED = 9, /* shape or option not built for sm_100a here               */
+  TSN_ERR_NOMEM = 10
+} tsn_status;
+
+/* Planner variants of the reference (pack once, CPU). */
+enum {
+  TSN_PLANNER_OPTIMIZED = 0, /* optimized_split24_pack  src/export_torchkbnufft_gpu_case.py:270-299 */
+  TSN_PLANNER_FAST = 1,      /* fast_split24_pack       src/export_torchkbnufft_gpu_case.py:46-99   */
+  TSN_PLANNER_SEARCH = 2     /* pack_view               src/nufft_layout_oracle.py:445-497          */
+};
+/* Row-grouping policies, src/nufft_layout_oracle.py:243-309. */
+enum { TSN_POLICY_TRAJECTORY = 0, TSN_POLICY_MORTON = 1, TSN_POLICY_OVERLAP = 2, TSN_POLICY_PACKING256 = 3 };
+/* Illegal-tile handling, src/export_gpu_case.py:110-155. */
+enum { TSN_ILLEGAL_SPLIT24 = 0, TSN_ILLEGAL_CSR_RESIDUAL = 1 };
+/* Views. */
+enum { TSN_VIEW_G = 0, TSN_VIEW_GT = 1 };
+/* Interpolation kernel choice. */
+enum { TSN_INTERP_AUTO = 0, TSN_INTERP_MMA_SP = 1, TSN_INTERP_TCGEN05 = 2 };
+/* Plan flags. */
+enum {
+  TSN_FLAG_REFERENCE_LAYOUT = 1 << 0 /* complex real/imag packs, image at [0,N) (reference pack format);
+                                        default for trajectory plans is the real-coefficient pack
+                                        with the image centred on the grid (same operator, half the
+                                        coefficient bytes) */
+};
+
+typedef struct tsn_plan_desc {
+  int32_t im_size;      /* N  (reference: kImage = 256, nufft_integrated_bench.cu:111)   */
+  int32_t grid_size;    /* G  (kGrid = 512)                                              */
+  int32_t coils;        /* C  (kCoils = 8), multiple of 4, <= 16                         */
+  int32_t kernel_width; /* J  (numpoints = 6)                                            */
+  int32_t planner;      /* TSN_PLANNER_*                                                 */
+  int32_t policy;       /* TSN_POLICY_*  (production: morton, run_fast_planner_matrix.py) */
+  uint64_t seed;        /* planner seed (20260823)                                       */
+  int32_t threads;      /* planner threads, 0 = all host cores                           */
+  int32_t flags;        /* TSN_FLAG_*                                                    */
+  int32_t interp;       /* TSN_INTERP_*                                                  */
+  int32_t device;       /* CUDA device ordinal the plan lives on (made current at every call) */
+  int32_t reserved[6];
+} tsn_plan_desc;
+
+typedef struct tsn_plan_info {
+  int64_t samples;            /* M                                           */
+  int32_t im_size, grid_size, coils, kernel_width, components;
+  int64_t groups[2], tiles[2], active_rows[2], nnz[2]; /* [TSN_VIEW_G], [TSN_VIEW_GT] */
+  int64_t pack_bytes[2];      /* device bytes of each view's pack              */
+  int64_t workspace_bytes;    /* device workspace owned by the plan            */
+  double plan_seconds;        /* host planner wall time                        */
+  int32_t interp;             /* kernel actually used (TSN_INTERP_MMA_SP / _TCGEN05) */
+  int32_t reserved[7];
+} tsn_plan_info;
+
+typedef struct tsn_cg_status {
+  int32_t completed_iterations;
+  int32_t positive_curvature;  /* 1 unless a denominator was <= 0 or non-finite   */
+  int32_t finite;              /* 1 unless the solution / residual went non-finite */
+  int32_t timeout;
+  double residual0, residual_final;
+} tsn_cg_status;
+
+typedef struct tsn_plan tsn_plan;
+
+/* ---- library ------------------------------------------------------------------------ */
+const char* tsn_version(void);
+/* Thread-local text of the last error (never NULL). */
+const char* tsn_get_last_error_string(void);
+tsn_status tsn_plan_desc_default(tsn_plan_desc* desc);
+
+/* ---- pack once (CPU) ------------------------------------------------------------------ */
+/* Complex KB interpolation matrix of a trajectory as CSR (rows = samples, columns sorted,
+ * exact zeros dropped).  Replaces tkbn.calc_tensor_spmatrix at
+ * src/export_torchkbnufft_gpu_case.py:537-567.  Two-call pattern: pass cols == NULL to get
+ * *nnz, then call again with arrays of that size.  row_ptr has m+1 entries. */
+tsn_status tsn_kb_interpolation_csr(const float* traj_cycles, int64_t m, int32_t im_size,
+                                    int32_t grid_size, int32_t width, int64_t* row_ptr,
+                                    int64_t* cols, double* re, double* im, int64_t* nnz);
+/* [N][N] deapodization table (the scaling.f32.bin role, export_real_runtime_inputs.py:97-101). */
+tsn_status tsn_kb_deapodization(int32_t im_size, int32_t grid_size, int32_t width, double* out);
+
+/* Pack one view of a complex sparse matrix given as CSR over samples (G) and write the
+ * production directories out_dir/real and out_dir/imag (packed_header_v2 + six arrays +
+ * manifest.json).  The structure (ones) is packed once and both components are placed on
+ * it — src/export_torchkbnufft_gpu_case.py:513-646 with --production-only. */
+tsn_status tsn_pack_csr_to_dirs(const int64_t* row_ptr, const int64_t* cols, const double* re,
+                                const double* im, int64_t rows, int32_t grid_size,
+                                const float* traj_cycles, int32_t view, int32_t planner,
+                                int32_t policy, uint64_t seed, int32_t threads,
+                                const char* out_dir);
+
+/* One real view packed like pack_view / fast / optimized, returned as raw tiles for parity
+ * checks against src/nufft_layout_oracle.py:445-497.  coords [rows][2] drive morton order.
+ * Two-call pattern on *tile_count (pass row_ids == NULL first).  row_ids [T][16],
+ * col_ids [T][k_tile], values [T][16][k_tile], legal [T]. */
+tsn_status tsn_pack_view_tiles(const int64_t* row_ptr, const int64_t* cols, const double* vals,
+                               const int64_t* logical_row_ids, const double* coords,
+                               int64_t rows, int64_t output_size, int64_t n_cols, int32_t planner,
+                               int32_t policy, int32_t k_tile, uint64_t seed, int32_t threads,
+                               int64_t* tile_count, int32_t* row_ids, int32_t* col_ids,
+                               double* values, uint8_t* legal);
+
+/* export_case (src/export_gpu_case.py:171-321) arrays for one real view, either illegal
+ * mode: writes header.bin, group_offsets.bin, group_row_ids.bin, tile_col_ids.bin,
+ * tile_a_comp.bin, tile_pair_meta.bin, residual_{row_ptr,cols,vals}.bin into out_dir. */
+tsn_status tsn_export_view_dir(const int64_t* row_ptr, const int64_t* cols, const double* vals,
+                               const int64_t* logical_row_ids, const double* coords, int64_t rows,
+                               int64_t output_size, int64_t n_cols, int32_t planner, int32_t policy,
+                               uint64_t seed, int32_t illegal_mode, int32_t threads,
+                               const char* out_dir);
+
+/* ---- plans (device residency) --------------------------------------------------------- */
+/* Load the four reference pack directories (load_direction x2, nufft_integrated_bench.cu:
+ * 135-226, same header/structure checks) plus an [N][N] deapodization table (host, may be
+ * NULL to use the KB table of desc).  Replaces the FWD_REAL FWD_IMAG ADJ_REAL ADJ_IMAG argv
+ * of nufft_fp16x2_cg_bench.cu:279-297. */
+tsn_status tsn_plan_create_from_pack(const char* fwd_real_dir, const char* fwd_imag_dir,
+                                     const char* adj_real_dir, const char* adj_imag_dir,
+                                     const float* scaling, const tsn_plan_desc* desc,
+                                     tsn_plan** plan);
+/* Build both packs from a trajectory with the C++ planner (pack once) and upload them. */
+tsn_status tsn_plan_create_from_trajectory(const float* traj_cycles, int64_t m,
+                                           const tsn_plan_desc* desc, tsn_plan** plan);
+tsn_status tsn_plan_destroy(tsn_plan* plan);
+tsn_status tsn_plan_get_info(const tsn_plan* plan, tsn_plan_info* info);
+
+/* ---- operators (device pointers, asynchronous on stream) ------------------------------ */
+/* y[C][M] = A x.  With smaps != NULL, x is the image [N][N] and the coil images are x*S_c
+ * (jkf_launch_custom_fft_f30_forward_sense_split2 + forward fused interpolation,
+ * nufft_integrated_bench.cu:527-585,604-627); with smaps == NULL, x is coil images [C][N][N]
+ * (jkf_launch_custom_fft_f30_forward_split2).  Unnormalized NUFFT units. */
+tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y,
+                       tsn_stream_t stream);
+/* x = A^H y: [N][N] coil-combined when smaps != NULL (launch_adjoint_image,
+ * nufft_fp16x2_cg_bench.cu:203-222, without the Tikhonov term), else coil images [C][N][N]. */
+tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x,
+                       tsn_stream_t stream);
+/* CG-SENSE on (A^H W A + lambda) x = A^H W y from x0 = 0, operator divided by operator_scale
+ * (launch_cg, nufft_fp16x2_cg_bench.cu:241-268; reference_sparse_solver.py cg_sense).
+ * density (W, [M]) may be NULL.  The whole solve runs as one CUDA graph (captured on first
+ * use per argument set).  residual_history (host, iters+1 entries) and status may be NULL;
+ * when either is given the call synchronizes the stream to fill them. */
+tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const float* density,
+                        float lambda, float operator_scale, int32_t iters, void* x,
+                        double* residual_history, tsn_cg_status* status, tsn_stream_t stream);
+
+/* ---- raw interpolation (parity with the reference GPU gate) --------------------------- */
+/* out[rows][16] f32 = component(view) x dense[n_cols][16] f16 for one real/imag component of
+ * a plan built from packs: the nufft_gt_spmma_*_f16_f32 contract checked against
+ * reference.bin (nufft_spmma_bench.cu:1090-1109).  component 0 = real, 1 = imag. */
+tsn_status tsn_interp_component(tsn_plan* plan, int32_t view, int32_t component,
+                                const void* dense_f16, float* out, tsn_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRAJSPARSENUFFT_H_ */

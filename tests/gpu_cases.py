@@ -1,0 +1,67 @@
+"""Seeded GPU test cases and oracle helpers (tests only)."""
+from __future__ import annotations
+
+import functools
+import math
+
+import numpy as np
+
+from oracle import nudft as onudft
+from oracle import operator as oop
+from trajsparsenufft_b200 import synth
+
+SEED = synth.BASE_SEED
+
+
+@functools.lru_cache(maxsize=None)
+def case(name: str):
+    """(trajectory, image, smaps, N, G, C, J, readout) of a named configuration."""
+    if name == "small":
+        n, g, c, spokes, readout = 64, 128, 4, 48, 128
+    elif name == "cfg0":          # 128^2, 4 coils, 96 x 256 golden-angle radial
+        n, g, c, spokes, readout = 128, 256, 4, 96, 256
+    elif name == "headline":      # 256^2, 8 coils, 256 x 512 golden-angle radial
+        n, g, c, spokes, readout = 256, 512, 8, 256, 512
+    elif name == "c16":
+        n, g, c, spokes, readout = 128, 256, 16, 64, 256
+    else:
+        raise KeyError(name)
+    traj = synth.golden_radial(spokes, readout)
+    x = synth.ellipse_phantom(n, SEED)
+    s = synth.coil_maps(n, c, SEED)
+    return traj, x, s, n, g, c, 6, readout
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def oracle_cg(forward, adjoint, y, density, iters, lam):
+    w = None if density is None else np.asarray(density, dtype=np.float64)
+    adj = adjoint if w is None else (lambda v: adjoint(w[None] * v))
+    return oop.cg_sense(forward, adj, y, iters, lam)
+
+
+@functools.lru_cache(maxsize=None)
+def measurement(name: str):
+    """FP64 NUDFT k-space + 1e-3 rms complex noise (BASELINE config 0 recipe)."""
+    traj, x, s, n, *_ = case(name)
+    if name == "headline":
+        # exact NUDFT at 131072 x 65536 x 8 is minutes on CPU; an FP64 KB NUFFT with
+        # J = 6 is within 3e-6 of it (checked at cfg0 in test_oracle_accuracy) and is
+        # used for data generation only
+        op = oop.KbSenseOperator(traj, n, 2 * n, 6, workers=8)
+        y = op.forward(x, s)
+    else:
+        y = onudft.Nudft(traj, n).forward(x, s)
+    return synth.add_noise(y, SEED)
+
+
+def torch_inputs(name: str, dev="cuda"):
+    import torch
+    traj, x, s, *_ = case(name)
+    y = measurement(name)
+    return (torch.from_numpy(np.ascontiguousarray(x)).to(dev), torch.from_numpy(np.ascontiguousarray(s)).to(dev),
+            torch.from_numpy(np.ascontiguousarray(y)).to(dev))

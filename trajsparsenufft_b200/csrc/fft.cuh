@@ -1,0 +1,169 @@
+// Warp-level FFT of length G = 32*P (P in {4, 8, 16, 32}) in FP32 registers.
+//
+// One warp transforms one G-point sequence held as P values per lane
+// (lane l, register j <-> element l + 32 j). Four-step decomposition G = P x 32:
+//   1. P-point DFT over j in registers (radix-2 DIT, compile-time twiddles),
+//   2. twiddle W_G^(l k),
+//   3. transpose through a padded per-warp shared buffer,
+//   4. 32-point DFTs over l, each split across T = 32/P lanes: a P-point register DFT
+//      per lane, twiddle W_32^(h m), then a T-point DFT across the T lanes by shuffles.
+// Output: lane (k = lane / T, h = lane % T) holds X[k + P m + P^2 h] in register m.
+// Forward = exp(-2 pi i nk/G), inverse = exp(+2 pi i nk/G), both unnormalized.
+// Twiddles are FP64-computed, FP32-stored tables (host fills them once per plan).
+// The reference's FFT endpoints are SIMT FP32 shared-memory radix-8/16/32 kernels
+// (nufft_custom_fft_forward_bench.cu:918-999, :1463-1552); this is an independent design.
+#pragma once
+
+#include "device.cuh"
+
+namespace tsn {
+namespace dev {
+
+// exp(-2 pi i e / 1024), e in [0, 1024); defined here, filled once per process by the host.
+// (included by exactly one translation unit)
+__constant__ float2 c_w1024[1024];
+
+template <bool INV>
+__device__ __forceinline__ float2 const_twiddle(int e1024) {
+  const float2 w = c_w1024[e1024 & 1023];
+  return INV ? make_float2(w.x, -w.y) : w;
+}
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+__host__ __device__ constexpr int bitrev(int x, int bits) {
+  return bits == 0 ? 0 : (((x & 1) << (bits - 1)) | bitrev(x >> 1, bits - 1));
+}
+
+// In-register DFT of length P (power of two), natural order in and out.
+template <int P, bool INV>
+__device__ __forceinline__ void dft_reg(float2 (&a)[P]) {
+  constexpr int L = ilog2(P);
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const int j = bitrev(i, L);
+    if (j > i) {
+      const float2 t = a[i];
+      a[i] = a[j];
+      a[j] = t;
+    }
+  }
+#pragma unroll
+  for (int s = 1; s <= L; ++s) {
+    const int len = 1 << s;
+    const int half = len >> 1;
+#pragma unroll
+    for (int i = 0; i < P; i += len) {
+#pragma unroll
+      for (int j = 0; j < half; ++j) {
+        const float2 u = a[i + j];
+        float2 t = a[i + j + half];
+        if (j != 0) {
+          if (4 * j == len) {  // W_len^(len/4) = -i (forward) / +i (inverse)
+            t = INV ? make_float2(-t.y, t.x) : make_float2(t.y, -t.x);
+          } else {
+            t = cmul(const_twiddle<INV>(j * (1024 / len)), t);
+          }
+        }
+        a[i + j] = cadd(u, t);
+        a[i + j + half] = csub(u, t);
+      }
+    }
+  }
+}
+
+template <int G>
+struct WarpFftShape {
+  static constexpr int P = G / 32;
+  static constexpr int T = 32 / P;
+  static constexpr int PITCH = 32 + T;        // padded row pitch (float2) of the transpose buffer
+  static constexpr int SCRATCH = P * PITCH;   // float2 per warp
+  static_assert(P * 32 == G && (P & (P - 1)) == 0 && P >= 4 && P <= 32, "G must be 32*P, P in {4..32}");
+};
+
+// tw: shared table exp(-2 pi i e / G), e in [0, G).
+template <int G, bool INV>
+__device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, const float2* tw) {
+  using S = WarpFftShape<G>;
+  constexpr int P = S::P, T = S::T;
+  const int lane = threadIdx.x & 31;
+  dft_reg<P, INV>(v);
+#pragma unroll
+  for (int k = 1; k < P; ++k) {
+    float2 w = tw[(lane * k) & (G - 1)];
+    if (INV) w.y = -w.y;
+    v[k] = cmul(v[k], w);
+  }
+#pragma unroll
+  for (int k = 0; k < P; ++k) scratch[k * S::PITCH + lane] = v[k];
+  __syncwarp();
+  const int kk = lane / T, h = lane % T;
+#pragma unroll
+  for (int i = 0; i < P; ++i) v[i] = scratch[kk * S::PITCH + T * i + h];
+  __syncwarp();
+  dft_reg<P, INV>(v);
+  if (T > 1) {
+#pragma unroll
+    for (int m = 1; m < P; ++m) {
+      float2 w = tw[(h * m * P) & (G - 1)];
+      if (INV) w.y = -w.y;
+      v[m] = cmul(v[m], w);
+    }
+    if (T == 2) {
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        float2 o;
+        o.x = __shfl_xor_sync(0xFFFFFFFFu, v[m].x, 1);
+        o.y = __shfl_xor_sync(0xFFFFFFFFu, v[m].y, 1);
+        v[m] = h == 0 ? cadd(v[m], o) : csub(o, v[m]);
+      }
+    } else if (T == 4) {
+      // X_h = sum_{h2} Z_{h2} W_4^{h2 h}, W_4 = -i (forward) / +i (inverse)
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        float2 z[4];
+#pragma unroll
+        for (int h2 = 0; h2 < 4; ++h2) {
+          z[h2].x = __shfl_sync(0xFFFFFFFFu, v[m].x, (lane & ~3) | h2);
+          z[h2].y = __shfl_sync(0xFFFFFFFFu, v[m].y, (lane & ~3) | h2);
+        }
+        const float2 s02 = cadd(z[0], z[2]), d02 = csub(z[0], z[2]);
+        const float2 s13 = cadd(z[1], z[3]), d13 = csub(z[1], z[3]);
+        // forward: X1 = d02 - i d13, X3 = d02 + i d13 ; inverse swaps
+        const float2 mi_d13 = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
+        float2 r;
+        if (h == 0) r = cadd(s02, s13);
+        else if (h == 1) r = cadd(d02, mi_d13);
+        else if (h == 2) r = csub(s02, s13);
+        else r = csub(d02, mi_d13);
+        v[m] = r;
+      }
+    } else {
+      // T == 8 (P == 4): radix-8 across lanes by direct summation
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int h2 = 0; h2 < 8; ++h2) {
+          float2 z;
+          z.x = __shfl_sync(0xFFFFFFFFu, v[m].x, (lane & ~7) | h2);
+          z.y = __shfl_sync(0xFFFFFFFFu, v[m].y, (lane & ~7) | h2);
+          float2 w = tw[((h2 * h) & 7) * (G / 8)];
+          if (INV) w.y = -w.y;
+          acc = cadd(acc, cmul(z, w));
+        }
+        v[m] = acc;
+      }
+    }
+  }
+}
+
+// Output element index held in register m after warp_fft.
+template <int G>
+__device__ __forceinline__ int warp_fft_out_index(int m) {
+  using S = WarpFftShape<G>;
+  const int lane = threadIdx.x & 31;
+  return lane / S::T + S::P * m + S::P * S::P * (lane % S::T);
+}
+
+}  // namespace dev
+}  // namespace tsn

@@ -1,0 +1,99 @@
+// Kernel argument structs and launchers of the sm_100a operator pipeline.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tsn {
+
+constexpr int kMaxCgIter = 256;
+constexpr int kNormParts = 296;      // 2 x 148 SMs
+constexpr float kPanelTarget = 8.0f; // rms target of the FP16 panels (power-of-two scaling)
+
+// Device scalar state of one solve (FP64 CG scalars, per-iteration panel scales).
+struct CgState {
+  double rho[kMaxCgIter + 2];    // <r_k, r_k>
+  double pap[kMaxCgIter + 1];    // Re <p_k, A p_k>
+  double alpha[kMaxCgIter + 1];
+  double beta[kMaxCgIter + 1];
+  float sigma[kMaxCgIter + 2];   // forward panel scale of p_k
+  float sigma_y;                 // sample panel scale of the measurement / adjoint input
+  float sigma_x;                 // forward panel scale of a plain forward call
+  int curvature_ok;
+  int finite_ok;
+  int completed;
+  int pad_;
+};
+
+// Interpolation view on the device: AoS tile records
+//   [0,128)            int32 col ids (internal panel row index)
+//   [128+576c, +512)   f16 compressed A of component c, [16][16]
+//   [640+576c, +64)    u32 mma.sp pair metadata of component c, [16]
+struct InterpView {
+  const uint8_t* records = nullptr;
+  const uint32_t* group_offsets = nullptr;
+  const int32_t* group_rows = nullptr;  // internal row id, -1 pad
+  int32_t groups = 0;
+  int32_t ncomp = 0;
+  int32_t rec_bytes = 0;
+};
+
+enum InterpEpilogue { EPI_SAMPLES = 0, EPI_GRID = 1, EPI_PANEL = 2, EPI_RAW = 3 };
+
+struct InterpOut {
+  float2* c64 = nullptr;          // EPI_SAMPLES: [C][rows]; EPI_GRID: [rows][C]
+  __half* panel = nullptr;        // EPI_PANEL: [rows][4C] (hi | res, interleaved complex)
+  float* raw = nullptr;           // EPI_RAW: [rows][16]
+  const float* density = nullptr; // EPI_PANEL weight per row
+  const float* scale_ptr = nullptr;  // device scalar (nullable)
+  int scale_inv = 0;              // use 1/(*scale_ptr)
+  float scale_mul = 1.0f;
+  int64_t rows = 0;               // row count (coil stride for EPI_SAMPLES)
+  int32_t coils = 0;
+};
+
+struct FftArgs {
+  int N = 0, G = 0, C = 0, shift = 0;   // grid position n holds image index (n + shift) mod G
+  const float2* tw = nullptr;           // exp(-2 pi i e/G), e in [0,G)
+  const float* scaling = nullptr;       // [N][N] deapodization
+  const float2* smaps = nullptr;        // [C][N][N] or null
+};
+
+void set_twiddle_constants(cudaStream_t s);
+
+void launch_interp(const InterpView& v, const __half* panel, int rowh, bool split, int epi, bool conj,
+                   const InterpOut& o, cudaStream_t s);
+
+void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t s);
+
+// forward rows: x (image [N][N] with smaps, coil images [C][N][N] without) -> z1 [G][N][C]
+// mode 0: plain, sigma from norm partials -> state->sigma_x
+// mode 1: CG iteration k: p = r + beta p (p = r at k == 0), rho_k from rr partials
+void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
+                     const double* partials, int nparts, CgState* st, int iter, cudaStream_t s);
+// forward columns: z1 -> panel [G*G][4C] (row q1*G + q0), FP16 hi | res
+void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStream_t s);
+// samples [C][M] (scaled by sigma_y, density) -> sample panel [M][4C]
+void launch_split_samples(const float2* y, const float* density, int64_t m, int c, __half* panel,
+                          const double* partials, int nparts, CgState* st, cudaStream_t s);
+// inverse columns: grid [G*G][C] -> w1 [G][N][C]
+void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStream_t s);
+// inverse rows + crop + deapod + coil combine
+// mode 0: plain adjoint (factor 1/sigma_y): out = [N][N] (smaps) or [C][N][N]
+// mode 1: CG RHS: r = b, x = 0, rr partials
+// mode 2: CG iteration k: ap = factor*AHAp + lambda p, pap partials
+void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r,
+                     const float2* p, double* partials, CgState* st, int iter, float inv_scale2,
+                     float lambda_scaled, cudaStream_t s);
+// CG update: x += alpha p, r -= alpha ap, rr partials
+void launch_cg_update(int N, float2* x, float2* r, const float2* p, const float2* ap, const double* pap_parts,
+                      double* rr_parts, CgState* st, int iter, cudaStream_t s);
+void launch_cg_finish(int N, const double* rr_parts, CgState* st, int iters, cudaStream_t s);
+
+void launch_gather_rows_f16(const __half* src, const int32_t* map, int64_t rows, int width, __half* dst,
+                            cudaStream_t s);
+void launch_gather_rows_f32(const float* src, const int32_t* map, int64_t rows, int width, float* dst,
+                            cudaStream_t s);
+
+}  // namespace tsn

@@ -1,0 +1,664 @@
+// Plans (device-resident packs + workspaces) and the device-side C ABI:
+// tsn_plan_create_from_pack / _from_trajectory, tsn_forward, tsn_adjoint, tsn_cg_sense,
+// tsn_interp_component. Replaces load_direction + launch_integrated_once + launch_cg of
+// experiments/production/src/nufft_integrated_bench.cu:135-226, :604-674 and
+// nufft_fp16x2_cg_bench.cu:203-268 with one plan object and one CUDA graph per solve.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "kb.hpp"
+#include "kernels.cuh"
+#include "pack_io.hpp"
+#include "planner.hpp"
+
+using namespace tsn;
+
+#define CUDA_OK(expr)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) fail(TSN_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace tsn {
+tsn_status guard_status(const std::exception& e);
+}
+
+namespace {
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() {
+    if (ptr) cudaFree(ptr);
+  }
+  void alloc(size_t n) {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = n;
+    if (n) CUDA_OK(cudaMalloc(&ptr, n));
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+  template <class T>
+  void upload(const std::vector<T>& v) {
+    alloc(v.size() * sizeof(T));
+    if (!v.empty()) CUDA_OK(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+};
+
+// Host image of one view before upload (reference index space).
+struct HostView {
+  int64_t output_size = 0, n_cols = 0, active_rows = 0, nnz = 0;
+  std::vector<uint32_t> group_offsets;
+  std::vector<int32_t> group_row_ids;  // reference row ids
+  std::vector<int32_t> tile_col_ids;   // reference col ids
+  std::vector<std::vector<uint16_t>> a;     // per component [tiles][16][16]
+  std::vector<std::vector<uint32_t>> meta;  // per component [tiles][16] pair layout
+  int64_t tiles() const { return static_cast<int64_t>(tile_col_ids.size() / kKTile); }
+  int64_t groups() const { return static_cast<int64_t>(group_offsets.size()) - 1; }
+};
+
+struct DevView {
+  DeviceBuffer records, offsets, rows;
+  InterpView v;
+  int64_t tiles = 0, groups = 0, active_rows = 0, nnz = 0, output_size = 0, n_cols = 0;
+  bool present = false;
+};
+
+struct GraphKey {
+  const void *y, *smaps, *density, *x;
+  int iters;
+  uint32_t lam_bits, scale_bits;
+  cudaStream_t stream;
+  bool operator<(const GraphKey& o) const {
+    return std::tie(y, smaps, density, x, iters, lam_bits, scale_bits, stream) <
+           std::tie(o.y, o.smaps, o.density, o.x, o.iters, o.lam_bits, o.scale_bits, o.stream);
+  }
+};
+
+std::once_flag g_const_once;
+
+}  // namespace
+
+struct tsn_plan {
+  tsn_plan_desc desc{};
+  int N = 0, G = 0, C = 0, J = 0, ncomp = 0, shift = 0, rowh = 0;
+  int64_t M = 0;
+  DevView view[2];
+  DeviceBuffer scaling, tw, z1, panel, spanel, grid, r, p, ap, parts_pap, parts_rr, norm_parts, state;
+  tsn_plan_info info{};
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  ~tsn_plan() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  }
+};
+
+namespace {
+
+// reference cell index q0*G + q1 -> internal q1*G + q0
+inline int64_t cell_to_internal(int64_t q, int64_t g) { return (q % g) * g + q / g; }
+
+void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
+  DevView& d = P->view[which];
+  const int64_t tiles = h.tiles(), groups = h.groups();
+  const int ncomp = static_cast<int>(h.a.size());
+  const int rec = 128 + 576 * ncomp;
+  std::vector<uint8_t> records(static_cast<size_t>(tiles) * rec, 0);
+  for (int64_t t = 0; t < tiles; ++t) {
+    uint8_t* r = records.data() + t * rec;
+    int32_t cols[kKTile];
+    for (int j = 0; j < kKTile; ++j) {
+      int64_t c = h.tile_col_ids[t * kKTile + j];
+      if (cols_are_cells) c = cell_to_internal(c, P->G);
+      cols[j] = static_cast<int32_t>(c);
+    }
+    std::memcpy(r, cols, sizeof cols);
+    for (int c = 0; c < ncomp; ++c) {
+      std::memcpy(r + 128 + 576 * c, &h.a[c][t * 256], 512);
+      std::memcpy(r + 640 + 576 * c, &h.meta[c][t * 16], 64);
+    }
+  }
+  std::vector<int32_t> rows(h.group_row_ids.size());
+  for (size_t i = 0; i < rows.size(); ++i) {
+    const int32_t v = h.group_row_ids[i];
+    rows[i] = (v >= 0 && rows_are_cells) ? static_cast<int32_t>(cell_to_internal(v, P->G)) : v;
+  }
+  d.records.upload(records);
+  d.offsets.upload(h.group_offsets);
+  d.rows.upload(rows);
+  d.v.records = d.records.as<uint8_t>();
+  d.v.group_offsets = d.offsets.as<uint32_t>();
+  d.v.group_rows = d.rows.as<int32_t>();
+  d.v.groups = static_cast<int32_t>(groups);
+  d.v.ncomp = ncomp;
+  d.v.rec_bytes = rec;
+  d.tiles = tiles;
+  d.groups = groups;
+  d.active_rows = h.active_rows;
+  d.nnz = h.nnz;
+  d.output_size = h.output_size;
+  d.n_cols = h.n_cols;
+  d.present = true;
+  P->info.groups[which] = groups;
+  P->info.tiles[which] = tiles;
+  P->info.active_rows[which] = h.active_rows;
+  P->info.nnz[which] = h.nnz;
+  P->info.pack_bytes[which] = static_cast<int64_t>(records.size() + h.group_offsets.size() * 4 + rows.size() * 4);
+}
+
+void check_desc(const tsn_plan_desc* d) {
+  if (!d) fail(TSN_ERR_ARG, "plan descriptor is NULL");
+  if (d->im_size <= 0 || d->im_size % 2 || d->grid_size < d->im_size) fail(TSN_ERR_SHAPE, "need an even image size <= grid size");
+  if (d->coils < 4 || d->coils > 16 || d->coils % 4) fail(TSN_ERR_UNSUPPORTED, "coil count must be 4, 8, 12 or 16");
+  if (d->kernel_width < 1 || d->kernel_width > 16) fail(TSN_ERR_ARG, "kernel width out of range");
+}
+
+// FFT endpoints are built for power-of-two grids of 128..1024 points.
+void need_fft(const tsn_plan* P) {
+  const int G = P->G;
+  if (G < 128 || G > 1024 || (G & (G - 1)))
+    fail(TSN_ERR_UNSUPPORTED, "FFT endpoints need a power-of-two grid size in [128, 1024]");
+}
+
+void allocate_workspaces(tsn_plan* P) {
+  const int64_t N = P->N, G = P->G, C = P->C, M = P->M;
+  P->rowh = static_cast<int>(4 * C);
+  std::vector<float2> tw(G);
+  for (int64_t e = 0; e < G; ++e) {
+    const double a = -2.0 * M_PI * static_cast<double>(e) / static_cast<double>(G);
+    tw[e] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+  }
+  P->tw.upload(tw);
+  P->z1.alloc(sizeof(float2) * G * N * C);
+  P->panel.alloc(sizeof(__half) * G * G * 4 * C);
+  P->spanel.alloc(sizeof(__half) * std::max<int64_t>(M, 1) * 4 * C);
+  P->grid.alloc(sizeof(float2) * G * G * C);
+  CUDA_OK(cudaMemset(P->grid.ptr, 0, P->grid.bytes));  // inactive grid rows stay zero
+  P->r.alloc(sizeof(float2) * N * N);
+  P->p.alloc(sizeof(float2) * N * N);
+  P->ap.alloc(sizeof(float2) * N * N);
+  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(N, kNormParts));
+  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(N, kNormParts));
+  P->norm_parts.alloc(sizeof(double) * kNormParts);
+  P->state.alloc(sizeof(CgState));
+  CUDA_OK(cudaMemset(P->state.ptr, 0, sizeof(CgState)));
+  P->info.workspace_bytes = static_cast<int64_t>(P->z1.bytes + P->panel.bytes + P->spanel.bytes + P->grid.bytes +
+                                                 3 * P->r.bytes + P->state.bytes);
+  std::call_once(g_const_once, []() { set_twiddle_constants(nullptr); });
+  CUDA_OK(cudaGetLastError());
+}
+
+FftArgs fft_args(const tsn_plan* P, const void* smaps) {
+  FftArgs f;
+  f.N = P->N;
+  f.G = P->G;
+  f.C = P->C;
+  f.shift = P->shift;
+  f.tw = P->tw.as<float2>();
+  f.scaling = P->scaling.as<float>();
+  f.smaps = static_cast<const float2*>(smaps);
+  return f;
+}
+
+HostView host_view_from_dirs(const char* real_dir, const char* imag_dir) {
+  const PackArrays re = read_pack_dir(real_dir);
+  HostView h;
+  h.output_size = re.h.output_size;
+  h.n_cols = re.h.n_cols;
+  h.active_rows = re.h.active_rows;
+  h.nnz = re.h.nnz;
+  if (re.h.residual_nnz != 0) fail(TSN_ERR_FORMAT, "incompatible packed direction: residual_nnz != 0");
+  h.group_offsets = re.group_offsets;
+  h.group_row_ids = re.group_row_ids;
+  h.tile_col_ids = re.tile_col_ids;
+  h.a.push_back(re.tile_a_comp);
+  h.meta.push_back(re.tile_pair_meta);
+  if (imag_dir) {
+    const PackArrays im = read_pack_dir(imag_dir);
+    // same checks as load_direction (nufft_integrated_bench.cu:141-194)
+    if (std::memcmp(&re.h, &im.h, sizeof(PackHeader)) != 0)
+      fail(TSN_ERR_FORMAT, "incompatible real/imag packed direction (headers differ)");
+    if (re.group_offsets != im.group_offsets || re.group_row_ids != im.group_row_ids ||
+        re.tile_col_ids != im.tile_col_ids)
+      fail(TSN_ERR_FORMAT, "real/imag structures differ");
+    h.a.push_back(im.tile_a_comp);
+    h.meta.push_back(im.tile_pair_meta);
+  }
+  return h;
+}
+
+HostView host_view_from_tiles(const SparseView& structure, const std::vector<const SparseView*>& comps,
+                              const tsn_plan_desc* d) {
+  const auto packed = pack_view(structure, d->planner, d->policy, kKTile, d->seed, d->threads);
+  const GroupedTiles gt = split_legal_and_residual(structure, packed, TSN_ILLEGAL_SPLIT24);
+  HostView h;
+  h.output_size = structure.output_size;
+  h.n_cols = structure.n_cols;
+  h.active_rows = structure.rows();
+  h.nnz = structure.nnz();
+  h.group_offsets = gt.group_offsets;
+  h.group_row_ids = gt.group_row_ids;
+  for (const SparseView* comp : comps) {
+    const CompressedTiles ct = compress_tiles(component_tiles(gt.tiles, *comp));
+    if (h.tile_col_ids.empty()) h.tile_col_ids = ct.col_ids;
+    h.a.push_back(ct.values);
+    h.meta.push_back(ct.pair_meta);
+  }
+  return h;
+}
+
+}  // namespace
+
+namespace tsn {
+
+// numpy.mod(x, g) for float64 (fmod with the sign of the divisor)
+double np_mod(double x, double g) {
+  double m = std::fmod(x, g);
+  if (m != 0.0) {
+    if ((g < 0) != (m < 0)) m += g;
+  } else {
+    m = std::copysign(0.0, g);
+  }
+  return m;
+}
+
+// G-view sparse structure over samples from a KB CSR, with the reference's morton coords
+// (np.mod(traj*G + G/2, G), src/export_torchkbnufft_gpu_case.py:550-553).
+SparseView sample_view(const std::vector<int64_t>& row_ptr, const std::vector<int64_t>& cols,
+                       const std::vector<double>& vals, const float* traj, int64_t m, int64_t g) {
+  SparseView v;
+  v.output_size = m;
+  v.n_cols = g * g;
+  v.row_ptr = row_ptr;
+  v.cols = cols;
+  v.vals = vals;
+  v.row_ids.resize(m);
+  v.coords.resize(2 * m);
+  for (int64_t i = 0; i < m; ++i) {
+    v.row_ids[i] = i;
+    v.coords[2 * i] = np_mod(static_cast<double>(traj[2 * i]) * g + g / 2.0, static_cast<double>(g));
+    v.coords[2 * i + 1] = np_mod(static_cast<double>(traj[2 * i + 1]) * g + g / 2.0, static_cast<double>(g));
+  }
+  return v;
+}
+
+}  // namespace tsn
+
+// ---- C ABI: plans -------------------------------------------------------------------------
+extern "C" {
+
+tsn_status tsn_plan_create_from_pack(const char* fwd_real, const char* fwd_imag, const char* adj_real,
+                                     const char* adj_imag, const float* scaling, const tsn_plan_desc* desc,
+                                     tsn_plan** out) {
+  try {
+    if (!out) fail(TSN_ERR_ARG, "plan output pointer is NULL");
+    *out = nullptr;
+    check_desc(desc);
+    if (!fwd_real && !adj_real) fail(TSN_ERR_ARG, "at least one view directory is required");
+    const auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<tsn_plan> P(new tsn_plan);
+    P->desc = *desc;
+    P->N = desc->im_size;
+    P->G = desc->grid_size;
+    P->C = desc->coils;
+    P->J = desc->kernel_width;
+    P->shift = 0;  // reference layout: image at [0, N)
+    const int64_t cells = static_cast<int64_t>(P->G) * P->G;
+    HostView hv[2];
+    if (fwd_real) {
+      hv[0] = host_view_from_dirs(fwd_real, fwd_imag);
+      if (hv[0].n_cols != cells) fail(TSN_ERR_SHAPE, "forward pack columns != grid_size^2");
+      P->M = hv[0].output_size;
+    }
+    if (adj_real) {
+      hv[1] = host_view_from_dirs(adj_real, adj_imag);
+      if (hv[1].output_size != cells) fail(TSN_ERR_SHAPE, "adjoint pack rows != grid_size^2");
+      if (fwd_real && hv[1].n_cols != P->M) fail(TSN_ERR_SHAPE, "forward output_size != adjoint n_cols");
+      P->M = hv[1].n_cols;
+    }
+    if (fwd_real && adj_real && hv[0].a.size() != hv[1].a.size())
+      fail(TSN_ERR_FORMAT, "forward and adjoint packs have different component counts");
+    P->ncomp = static_cast<int>((fwd_real ? hv[0] : hv[1]).a.size());
+    CUDA_OK(cudaSetDevice(desc->device));  // all host-side checks are done: touch the device now
+    std::vector<float> sc(static_cast<size_t>(P->N) * P->N);
+    if (scaling) {
+      std::memcpy(sc.data(), scaling, sc.size() * sizeof(float));
+    } else {
+      const auto d = deapodization(P->N, P->G, P->J);
+      for (size_t i = 0; i < sc.size(); ++i) sc[i] = static_cast<float>(d[i]);
+    }
+    P->scaling.upload(sc);
+    if (fwd_real) upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
+    if (adj_real) upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
+    allocate_workspaces(P.get());
+    P->info.samples = P->M;
+    P->info.im_size = P->N;
+    P->info.grid_size = P->G;
+    P->info.coils = P->C;
+    P->info.kernel_width = P->J;
+    P->info.components = P->ncomp;
+    P->info.interp = TSN_INTERP_MMA_SP;
+    P->info.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = P.release();
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const tsn_plan_desc* desc, tsn_plan** out) {
+  try {
+    if (!out || !traj) fail(TSN_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    check_desc(desc);
+    if (m <= 0) fail(TSN_ERR_SHAPE, "trajectory is empty");
+    const auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<tsn_plan> P(new tsn_plan);
+    P->desc = *desc;
+    P->N = desc->im_size;
+    P->G = desc->grid_size;
+    P->C = desc->coils;
+    P->J = desc->kernel_width;
+    P->M = m;
+    const bool reference_layout = (desc->flags & TSN_FLAG_REFERENCE_LAYOUT) != 0;
+    P->shift = reference_layout ? 0 : P->N / 2;
+    for (int64_t i = 0; i < 2 * m; ++i)
+      if (!std::isfinite(traj[i]) || std::fabs(traj[i]) > 0.500001f)
+        fail(TSN_ERR_ARG, "trajectory must use normalized [-0.5, 0.5] coordinates");
+    const KbCsr kb = kb_interpolation_csr(traj, m, P->N, P->G, P->J);
+    std::vector<double> ones(kb.cols.size(), 1.0), weights(kb.cols.size());
+    for (size_t i = 0; i < weights.size(); ++i) weights[i] = std::hypot(kb.re[i], kb.im[i]);
+    const SparseView st_g = sample_view(kb.row_ptr, kb.cols, ones, traj, m, P->G);
+    const SparseView st_gt = transpose_view(st_g, P->G);
+    HostView hv[2];
+    if (reference_layout) {
+      const SparseView re_g = sample_view(kb.row_ptr, kb.cols, kb.re, traj, m, P->G);
+      const SparseView im_g = sample_view(kb.row_ptr, kb.cols, kb.im, traj, m, P->G);
+      const SparseView re_gt = transpose_view(re_g, P->G), im_gt = transpose_view(im_g, P->G);
+      hv[0] = host_view_from_tiles(st_g, {&re_g, &im_g}, desc);
+      hv[1] = host_view_from_tiles(st_gt, {&re_gt, &im_gt}, desc);
+      P->ncomp = 2;
+    } else {
+      // centred image: the phase exp(2 pi i q c/G) moves into the FFT shift, coefficients are
+      // the real KB weights
+      const SparseView w_g = sample_view(kb.row_ptr, kb.cols, weights, traj, m, P->G);
+      const SparseView w_gt = transpose_view(w_g, P->G);
+      hv[0] = host_view_from_tiles(st_g, {&w_g}, desc);
+      hv[1] = host_view_from_tiles(st_gt, {&w_gt}, desc);
+      P->ncomp = 1;
+    }
+    const auto d = deapodization(P->N, P->G, P->J);
+    std::vector<float> sc(d.size());
+    for (size_t i = 0; i < sc.size(); ++i) sc[i] = static_cast<float>(d[i]);
+    CUDA_OK(cudaSetDevice(desc->device));
+    P->scaling.upload(sc);
+    P->info.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
+    upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
+    allocate_workspaces(P.get());
+    P->info.samples = P->M;
+    P->info.im_size = P->N;
+    P->info.grid_size = P->G;
+    P->info.coils = P->C;
+    P->info.kernel_width = P->J;
+    P->info.components = P->ncomp;
+    P->info.interp = TSN_INTERP_MMA_SP;
+    *out = P.release();
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_plan_destroy(tsn_plan* plan) {
+  if (plan) cudaSetDevice(plan->desc.device);
+  delete plan;
+  return TSN_OK;
+}
+
+tsn_status tsn_plan_get_info(const tsn_plan* plan, tsn_plan_info* info) {
+  if (!plan || !info) {
+    set_last_error("NULL argument");
+    return TSN_ERR_ARG;
+  }
+  *info = plan->info;
+  return TSN_OK;
+}
+
+}  // extern "C"
+
+// ---- operators ----------------------------------------------------------------------------
+namespace {
+
+void need_views(const tsn_plan* P, bool fwd, bool adj) {
+  need_fft(P);
+  CUDA_OK(cudaSetDevice(P->desc.device));
+  if ((fwd && !P->view[TSN_VIEW_G].present) || (adj && !P->view[TSN_VIEW_GT].present))
+    fail(TSN_ERR_ARG, "plan lacks the pack view this operator needs");
+}
+
+void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cudaStream_t s) {
+  const FftArgs f = fft_args(P, smaps);
+  CgState* st = P->state.as<CgState>();
+  const int64_t n = static_cast<int64_t>(P->N) * P->N * (smaps ? 1 : P->C);
+  launch_norm_partials(static_cast<const float2*>(x), n, P->norm_parts.as<double>(), s);
+  launch_fwd_rows(f, static_cast<const float2*>(x), P->z1.as<float2>(), 0, nullptr, nullptr, P->norm_parts.as<double>(),
+                  kNormParts, st, 0, s);
+  launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
+  InterpOut o;
+  o.c64 = static_cast<float2*>(y);
+  o.rows = P->M;
+  o.coils = P->C;
+  o.scale_ptr = &st->sigma_x;
+  o.scale_inv = 1;
+  o.scale_mul = static_cast<float>(P->G);
+  launch_interp(P->view[TSN_VIEW_G].v, P->panel.as<__half>(), P->rowh, true, EPI_SAMPLES, false, o, s);
+}
+
+void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cudaStream_t s) {
+  CgState* st = P->state.as<CgState>();
+  launch_norm_partials(static_cast<const float2*>(y), P->M * P->C, P->norm_parts.as<double>(), s);
+  launch_split_samples(static_cast<const float2*>(y), density, P->M, P->C, P->spanel.as<__half>(),
+                       P->norm_parts.as<double>(), kNormParts, st, s);
+  InterpOut o;
+  o.c64 = P->grid.as<float2>();
+  o.rows = static_cast<int64_t>(P->G) * P->G;
+  o.coils = P->C;
+  launch_interp(P->view[TSN_VIEW_GT].v, P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, o, s);
+}
+
+void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* density, float lambda, float scale,
+                int iters, void* x, cudaStream_t s) {
+  const FftArgs f = fft_args(P, smaps);
+  CgState* st = P->state.as<CgState>();
+  const float inv_s2 = 1.0f / (scale * scale);
+  const float lam = lambda * inv_s2;
+  float2* X = static_cast<float2*>(x);
+  float2 *R = P->r.as<float2>(), *Pv = P->p.as<float2>(), *AP = P->ap.as<float2>();
+  double *pap = P->parts_pap.as<double>(), *rr = P->parts_rr.as<double>();
+  enqueue_adjoint_grid(P, y, density, s);
+  launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
+  launch_inv_rows(f, P->z1.as<float2>(), nullptr, 1, X, R, nullptr, rr, st, 0, inv_s2, 0.f, s);
+  for (int k = 0; k < iters; ++k) {
+    launch_fwd_rows(f, nullptr, P->z1.as<float2>(), 1, Pv, R, rr, P->N, st, k, s);
+    launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
+    InterpOut of;
+    of.panel = P->spanel.as<__half>();
+    of.density = density;
+    of.rows = P->M;
+    of.coils = P->C;
+    launch_interp(P->view[TSN_VIEW_G].v, P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
+    InterpOut oa;
+    oa.c64 = P->grid.as<float2>();
+    oa.rows = static_cast<int64_t>(P->G) * P->G;
+    oa.coils = P->C;
+    launch_interp(P->view[TSN_VIEW_GT].v, P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
+    launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
+    launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, k, inv_s2, lam, s);
+    launch_cg_update(P->N, X, R, Pv, AP, pap, rr, st, k, s);
+  }
+  launch_cg_finish(P->N, rr, st, iters, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream) {
+  try {
+    if (!plan || !x || !y) fail(TSN_ERR_ARG, "NULL argument");
+    need_views(plan, true, false);
+    enqueue_forward(plan, x, smaps, y, reinterpret_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream) {
+  try {
+    if (!plan || !x || !y) fail(TSN_ERR_ARG, "NULL argument");
+    need_views(plan, false, true);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    enqueue_adjoint_grid(plan, y, nullptr, s);
+    const FftArgs f = fft_args(plan, smaps);
+    launch_inv_cols(f, plan->grid.as<float2>(), plan->z1.as<float2>(), s);
+    launch_inv_rows(f, plan->z1.as<float2>(), static_cast<float2*>(x), 0, nullptr, nullptr, nullptr, nullptr,
+                    plan->state.as<CgState>(), 0, 1.0f, 0.f, s);
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const float* density, float lambda,
+                        float operator_scale, int32_t iters, void* x, double* residual_history,
+                        tsn_cg_status* status, tsn_stream_t stream) {
+  try {
+    if (!plan || !y || !smaps || !x) fail(TSN_ERR_ARG, "NULL argument (y, smaps and x are required)");
+    if (iters < 0 || iters > kMaxCgIter) fail(TSN_ERR_ARG, "iteration count out of range");
+    if (!(operator_scale > 0.0f) || !std::isfinite(lambda)) fail(TSN_ERR_ARG, "invalid operator scale or lambda");
+    need_views(plan, true, true);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    GraphKey key{y, smaps, density, x, iters, 0, 0, s};
+    std::memcpy(&key.lam_bits, &lambda, 4);
+    std::memcpy(&key.scale_bits, &operator_scale, 4);
+    auto it = plan->graphs.find(key);
+    if (it == plan->graphs.end()) {
+      cudaStream_t cap = s;
+      bool own = false;
+      if (cap == nullptr) {  // the legacy stream cannot be captured: capture on a private stream
+        CUDA_OK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        own = true;
+      }
+      cudaGraph_t g = nullptr;
+      CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
+      enqueue_cg(plan, y, smaps, density, lambda, operator_scale, iters, x, cap);
+      const cudaError_t launch_err = cudaGetLastError();
+      const cudaError_t end_err = cudaStreamEndCapture(cap, &g);
+      if (own) cudaStreamDestroy(cap);
+      if (launch_err != cudaSuccess) fail(TSN_ERR_CUDA, cudaGetErrorString(launch_err));
+      if (end_err != cudaSuccess) fail(TSN_ERR_CUDA, cudaGetErrorString(end_err));
+      cudaGraphExec_t exec = nullptr;
+      const cudaError_t inst = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      if (inst != cudaSuccess) fail(TSN_ERR_CUDA, cudaGetErrorString(inst));
+      if (plan->graphs.size() >= 8) {
+        cudaGraphExecDestroy(plan->graphs.begin()->second);
+        plan->graphs.erase(plan->graphs.begin());
+      }
+      it = plan->graphs.emplace(key, exec).first;
+    }
+    CUDA_OK(cudaGraphLaunch(it->second, s));
+    if (residual_history || status) {
+      CgState host;
+      CUDA_OK(cudaMemcpyAsync(&host, plan->state.ptr, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+      CUDA_OK(cudaStreamSynchronize(s));
+      if (residual_history)
+        for (int k = 0; k <= iters; ++k) residual_history[k] = std::sqrt(std::max(host.rho[k], 0.0));
+      if (status) {
+        status->completed_iterations = host.completed;
+        status->positive_curvature = host.curvature_ok;
+        status->finite = host.finite_ok && std::isfinite(host.rho[iters]);
+        status->timeout = 0;
+        status->residual0 = std::sqrt(std::max(host.rho[0], 0.0));
+        status->residual_final = std::sqrt(std::max(host.rho[iters], 0.0));
+      }
+      if (!host.finite_ok || !std::isfinite(host.rho[iters])) fail(TSN_ERR_NONFINITE, "CG produced non-finite values");
+      if (!host.curvature_ok) fail(TSN_ERR_CURVATURE, "CG denominator <= 0 (positive_curvature = 0)");
+    }
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_interp_component(tsn_plan* plan, int32_t view, int32_t component, const void* dense_f16, float* out,
+                                tsn_stream_t stream) {
+  try {
+    if (!plan || !dense_f16 || !out) fail(TSN_ERR_ARG, "NULL argument");
+    if (view != TSN_VIEW_G && view != TSN_VIEW_GT) fail(TSN_ERR_ARG, "unknown view");
+    const DevView& d = plan->view[view];
+    if (!d.present) fail(TSN_ERR_ARG, "plan lacks this view");
+    CUDA_OK(cudaSetDevice(plan->desc.device));
+    if (component < 0 || component >= d.v.ncomp) fail(TSN_ERR_ARG, "component out of range");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int64_t G = plan->G;
+    // internal <-> reference index maps of this view
+    std::vector<int32_t> col_map(d.n_cols), row_map(d.output_size);
+    for (int64_t j = 0; j < d.n_cols; ++j)
+      col_map[j] = static_cast<int32_t>(view == TSN_VIEW_G ? cell_to_internal(j, G) : j);  // internal j <- ref
+    for (int64_t j = 0; j < d.output_size; ++j)
+      row_map[j] = static_cast<int32_t>(view == TSN_VIEW_GT ? cell_to_internal(j, G) : j);
+    DeviceBuffer cm, rm, din, dout;
+    cm.upload(col_map);
+    rm.upload(row_map);
+    din.alloc(sizeof(__half) * d.n_cols * 16);
+    dout.alloc(sizeof(float) * d.output_size * 16);
+    CUDA_OK(cudaMemsetAsync(dout.ptr, 0, dout.bytes, s));
+    // cell_to_internal is an involution on square grids: internal row j holds reference row map[j]
+    launch_gather_rows_f16(static_cast<const __half*>(dense_f16), cm.as<int32_t>(), d.n_cols, 16, din.as<__half>(), s);
+    InterpView v = d.v;
+    std::vector<uint8_t> dummy;
+    InterpOut o;
+    o.raw = dout.as<float>();
+    o.rows = d.output_size;
+    // component selection: records of component c start 576*c bytes later for A/meta
+    DeviceBuffer shifted;
+    if (component != 0) {
+      // build a single-component record copy for component 1
+      std::vector<uint8_t> host(static_cast<size_t>(d.tiles) * d.v.rec_bytes);
+      CUDA_OK(cudaMemcpy(host.data(), d.v.records, host.size(), cudaMemcpyDeviceToHost));
+      std::vector<uint8_t> one(static_cast<size_t>(d.tiles) * 704);
+      for (int64_t t = 0; t < d.tiles; ++t) {
+        std::memcpy(&one[t * 704], &host[t * d.v.rec_bytes], 128);
+        std::memcpy(&one[t * 704 + 128], &host[t * d.v.rec_bytes + 128 + 576], 576);
+      }
+      shifted.upload(one);
+      v.records = shifted.as<uint8_t>();
+      v.rec_bytes = 704;
+    }
+    v.ncomp = 1;
+    launch_interp(v, din.as<__half>(), 16, false, EPI_RAW, false, o, s);
+    launch_gather_rows_f32(dout.as<float>(), rm.as<int32_t>(), d.output_size, 16, out, s);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaStreamSynchronize(s));
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+}  // extern "C"

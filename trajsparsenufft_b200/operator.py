@@ -1,0 +1,215 @@
+"""Plans and operators: the Python face of the C ABI.
+
+``Plan`` mirrors what the reference CG binary assembles from its argv
+(nufft_fp16x2_cg_bench.cu:279-297: four pack directories, a runtime directory,
+the operator scale, the iteration count) plus the forward / adjoint operator
+pair of nufft_integrated_bench.cu:604-674.  Device memory and streams come from
+torch (plumbing only); every operator runs in the CUDA library, there is no
+CPU or torch fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from ._lib import CgStatus, PlanDesc, PlanInfo, check, lib, ptr
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_handle(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dev_ptr(t, dtype, shape, name):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} must have shape {tuple(shape)}, got {tuple(t.shape)}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return C.c_void_p(t.data_ptr())
+
+
+def plan_desc(im_size=256, grid_size=512, coils=8, width=6, planner="optimized", policy="morton",
+              seed=20260823, threads=0, reference_layout=False, device=None) -> PlanDesc:
+    d = PlanDesc()
+    check(lib().tsn_plan_desc_default(C.byref(d)))
+    d.im_size, d.grid_size, d.coils, d.kernel_width = im_size, grid_size, coils, width
+    d.planner, d.policy, d.seed, d.threads = _lib.PLANNER[planner], _lib.POLICY[policy], seed, threads
+    d.flags = _lib.FLAG_REFERENCE_LAYOUT if reference_layout else 0
+    if device is None:
+        try:
+            torch = _torch()
+            device = torch.cuda.current_device() if torch.cuda.is_available() else 0
+        except Exception:
+            device = 0
+    d.device = int(device)
+    return d
+
+
+class Plan:
+    """Device-resident forward/adjoint packs of one trajectory plus solver workspaces."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        info = PlanInfo()
+        check(lib().tsn_plan_get_info(self._h, C.byref(info)))
+        self.samples = info.samples
+        self.im_size = info.im_size
+        self.grid_size = info.grid_size
+        self.coils = info.coils
+        self.width = info.kernel_width
+        self.components = info.components
+        self.info = {
+            "samples": info.samples, "im_size": info.im_size, "grid_size": info.grid_size, "coils": info.coils,
+            "kernel_width": info.kernel_width, "components": info.components,
+            "groups": list(info.groups), "tiles": list(info.tiles), "active_rows": list(info.active_rows),
+            "nnz": list(info.nnz), "pack_bytes": list(info.pack_bytes), "workspace_bytes": info.workspace_bytes,
+            "plan_seconds": info.plan_seconds, "interp": info.interp,
+        }
+
+    # ---- construction ------------------------------------------------------------------
+    @classmethod
+    def from_trajectory(cls, trajectory, *, im_size=256, grid_size=512, coils=8, width=6, planner="optimized",
+                        policy="morton", seed=20260823, threads=0, reference_layout=False, device=None) -> "Plan":
+        t = np.ascontiguousarray(np.asarray(trajectory, dtype=np.float32).reshape(-1, 2))
+        d = plan_desc(im_size, grid_size, coils, width, planner, policy, seed, threads, reference_layout, device)
+        h = C.c_void_p()
+        check(lib().tsn_plan_create_from_trajectory(ptr(t, C.c_float), t.shape[0], C.byref(d), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_pack(cls, fwd_real, fwd_imag, adj_real, adj_imag, *, im_size=256, grid_size=512, coils=8, width=6,
+                  scaling=None, device=None) -> "Plan":
+        """Load reference-format pack directories (load_direction x 2)."""
+        enc = (lambda p: None if p is None else str(Path(p)).encode())
+        sc = None if scaling is None else np.ascontiguousarray(np.asarray(scaling, dtype=np.float32))
+        if sc is not None and sc.shape != (im_size, im_size):
+            raise ValueError("scaling must be [im_size, im_size]")
+        d = plan_desc(im_size, grid_size, coils, width, device=device)
+        h = C.c_void_p()
+        check(lib().tsn_plan_create_from_pack(enc(fwd_real), enc(fwd_imag), enc(adj_real), enc(adj_imag),
+                                              ptr(sc, C.c_float), C.byref(d), C.byref(h)))
+        return cls(h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().tsn_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- operators ------------------------------------------------------------------------
+    def _image_shape(self, smaps):
+        n = self.im_size
+        return (n, n) if smaps is not None else (self.coils, n, n)
+
+    def forward(self, x, smaps=None, out=None, stream=None):
+        """y[C, M] = A x (unnormalized NUFFT of x*S_c, or of coil images when smaps is None)."""
+        torch = _torch()
+        cf = torch.complex64
+        xp = _dev_ptr(x, cf, self._image_shape(smaps), "x")
+        sp = None if smaps is None else _dev_ptr(smaps, cf, (self.coils, self.im_size, self.im_size), "smaps")
+        if out is None:
+            out = torch.empty((self.coils, self.samples), dtype=cf, device=x.device)
+        yp = _dev_ptr(out, cf, (self.coils, self.samples), "out")
+        check(lib().tsn_forward(self._h, xp, sp, yp, _stream_handle(stream)))
+        return out
+
+    def adjoint(self, y, smaps=None, out=None, stream=None):
+        """x = A^H y: coil-combined image [N, N] with smaps, else coil images [C, N, N]."""
+        torch = _torch()
+        cf = torch.complex64
+        yp = _dev_ptr(y, cf, (self.coils, self.samples), "y")
+        sp = None if smaps is None else _dev_ptr(smaps, cf, (self.coils, self.im_size, self.im_size), "smaps")
+        if out is None:
+            out = torch.empty(self._image_shape(smaps), dtype=cf, device=y.device)
+        xp = _dev_ptr(out, cf, self._image_shape(smaps), "out")
+        check(lib().tsn_adjoint(self._h, yp, sp, xp, _stream_handle(stream)))
+        return out
+
+    def cg_sense(self, y, smaps, *, density=None, lam=1e-4, iters=10, operator_scale=1.0, out=None, stream=None,
+                 sync=True):
+        """CG-SENSE solve of (A^H W A + lam) x = A^H W y from x0 = 0 (one CUDA graph).
+
+        Returns (x, residual history or None, status dict or None).  With sync=False
+        the call is fully asynchronous and no host-side status is produced.
+        """
+        torch = _torch()
+        cf = torch.complex64
+        n = self.im_size
+        yp = _dev_ptr(y, cf, (self.coils, self.samples), "y")
+        sp = _dev_ptr(smaps, cf, (self.coils, n, n), "smaps")
+        dp = None if density is None else _dev_ptr(density, torch.float32, (self.samples,), "density")
+        if out is None:
+            out = torch.empty((n, n), dtype=cf, device=y.device)
+        xp = _dev_ptr(out, cf, (n, n), "out")
+        hist = np.zeros(iters + 1, dtype=np.float64) if sync else None
+        st = CgStatus() if sync else None
+        rc = lib().tsn_cg_sense(self._h, yp, sp, dp, float(lam), float(operator_scale), int(iters), xp,
+                                ptr(hist, C.c_double), C.byref(st) if sync else None, _stream_handle(stream))
+        status = None
+        if sync:
+            status = {"completed_iterations": st.completed_iterations,
+                      "positive_curvature": bool(st.positive_curvature), "finite": bool(st.finite),
+                      "timeout": bool(st.timeout), "residual0": st.residual0, "residual_final": st.residual_final}
+            if rc in (4, 5):  # NONFINITE / CURVATURE: reported in the status, x returned as computed
+                status["failure"] = _lib.STATUS[rc]
+                return out, hist, status
+        check(rc)
+        return out, hist, status
+
+    def interp_component(self, view: str, component: int, dense_f16):
+        """Raw out[rows,16] f32 = component(view) @ dense[n_cols,16] (reference.bin contract)."""
+        torch = _torch()
+        rows = self.grid_size ** 2 if view == "G_T" else self.samples
+        cols = self.samples if view == "G_T" else self.grid_size ** 2
+        dp = _dev_ptr(dense_f16, torch.float16, (cols, 16), "dense")
+        out = torch.zeros((rows, 16), dtype=torch.float32, device=dense_f16.device)
+        check(lib().tsn_interp_component(self._h, _lib.VIEW[view], int(component), dp, C.c_void_p(out.data_ptr()),
+                                         _stream_handle(None)))
+        return out
+
+
+def load_runtime_dir(directory, coils: int, im_size: int, samples: int) -> dict:
+    """Runtime inputs in the reference layout (export_real_runtime_inputs.py:97-113)."""
+    d = Path(directory)
+    out = {
+        "measurement": np.fromfile(d / "measurement.c64.bin", dtype=np.complex64).reshape(coils, samples),
+        "sensitivity_maps": np.fromfile(d / "sensitivity_maps.c64.bin", dtype=np.complex64).reshape(
+            coils, im_size, im_size),
+        "scaling": np.fromfile(d / "scaling.f32.bin", dtype=np.float32).reshape(im_size, im_size),
+    }
+    if (d / "density.f32.bin").exists():
+        out["density"] = np.fromfile(d / "density.f32.bin", dtype=np.float32).reshape(samples)
+    return out
+
+
+def write_runtime_dir(directory, measurement, sensitivity_maps, scaling, density=None, truth=None) -> Path:
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    np.ascontiguousarray(measurement, dtype=np.complex64).tofile(d / "measurement.c64.bin")
+    np.ascontiguousarray(sensitivity_maps, dtype=np.complex64).tofile(d / "sensitivity_maps.c64.bin")
+    np.ascontiguousarray(scaling, dtype=np.float32).tofile(d / "scaling.f32.bin")
+    if density is not None:
+        np.ascontiguousarray(density, dtype=np.float32).tofile(d / "density.f32.bin")
+    if truth is not None:
+        np.ascontiguousarray(truth, dtype=np.complex64).tofile(d / "truth.c64.bin")
+    return d
