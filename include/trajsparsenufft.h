@@ -190,6 +190,20 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
                         float lambda, float operator_scale, int32_t iters, void* x,
                         double* residual_history, tsn_cg_status* status, tsn_stream_t stream);
 
+/* ---- FFT endpoints (the role of nufft_custom_fft_f30_api.h:6-34) ---------------------- */
+/* Forward endpoint: panel[G*G][4C] f16 = s * FFT_G(pad(x * S_c * scaling)), rows q1*G + q0
+ * (q1-major), each row = FP16 high parts then FP16 residuals, (re, im) interleaved per coil;
+ * s is a power of two chosen from the input norm and written to *panel_scale (host; the
+ * call synchronizes when panel_scale != NULL).  Replaces
+ * jkf_launch_custom_fft_f30_forward_sense_split2 (x-stage + y-stage). */
+tsn_status tsn_fft_forward_panel(tsn_plan* plan, const void* x, const void* smaps, void* panel_f16,
+                                 float* panel_scale, tsn_stream_t stream);
+/* Adjoint endpoint: x = sum_c conj(S_c) * scaling * crop(IFFT_G(grid_c)) (unnormalized inverse)
+ * from grid[G*G][C] c64 with rows q1*G + q0; coil images [C][N][N] when smaps == NULL.
+ * Replaces jkf_launch_custom_ifft_f31_adjoint + sense_combine_scaled. */
+tsn_status tsn_fft_adjoint_image(tsn_plan* plan, const void* grid_c64, const void* smaps, void* x,
+                                 tsn_stream_t stream);
+
 /* ---- raw interpolation (parity with the reference GPU gate) --------------------------- */
 /* out[rows][16] f32 = component(view) x dense[n_cols][16] f16 for one real/imag component of
  * a plan built from packs: the nufft_gt_spmma_*_f16_f32 contract checked against

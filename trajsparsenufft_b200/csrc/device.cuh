@@ -68,19 +68,22 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Deterministic block sum of one double per thread (fixed reduction tree); result valid in
-// thread 0. `scratch` holds blockDim.x/32 doubles.
+// Deterministic block sum of one double per thread (fixed reduction tree), returned to
+// every thread. `scratch` holds 33 doubles.
 __device__ __forceinline__ double block_sum(double v, double* scratch) {
   v = warp_sum(v);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0) scratch[warp] = v;
   __syncthreads();
-  double t = 0.0;
   if (threadIdx.x == 0) {
     const int nw = (blockDim.x + 31) >> 5;
+    double t = 0.0;
     for (int w = 0; w < nw; ++w) t += scratch[w];
+    scratch[32] = t;
   }
   __syncthreads();
+  const double t = scratch[32];
+  __syncthreads();  // scratch may be reused by the caller's next block_sum
   return t;
 }
 

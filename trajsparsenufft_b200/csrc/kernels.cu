@@ -218,7 +218,7 @@ void launch_interp(const InterpView& v, const __half* panel, int rowh, bool spli
 // Reductions
 // ------------------------------------------------------------------------------------------
 __global__ void norm_partials_kernel(const float2* __restrict__ v, int64_t n, double* __restrict__ part) {
-  __shared__ double scratch[32];
+  __shared__ double scratch[33];
   double acc = 0.0;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -265,7 +265,7 @@ __global__ void fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2*
   float2* row_s = tw_s + G;                        // [N]
   float2* out_s = row_s + f.N;                     // [G][C]
   float2* scr = out_s + G * f.C;                   // [C][SCR]
-  __shared__ double red[32];
+  __shared__ double red[33];
   const int i0 = blockIdx.x, N = f.N, C = f.C;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
@@ -385,7 +385,7 @@ __global__ void fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1, __half
 __global__ void split_samples_kernel(const float2* __restrict__ y, const float* __restrict__ density, int64_t m,
                                      int C, __half* __restrict__ panel, const double* __restrict__ parts, int nparts,
                                      CgState* __restrict__ st) {
-  __shared__ double red[32];
+  __shared__ double red[33];
   const double total = sum_partials(parts, nparts, red);
   const float sigma = pow2_scale(total, static_cast<double>(m) * C, kPanelTarget);
   if (blockIdx.x == 0 && threadIdx.x == 0) st->sigma_y = sigma;
@@ -456,7 +456,7 @@ __global__ void inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2
   float2* in_s = tw_s + G;               // [G][C]
   float2* img_s = in_s + G * f.C;        // [C][N]
   float2* scr = img_s + f.N * f.C;       // [C][SCR]
-  __shared__ double red[32];
+  __shared__ double red[33];
   const int i0 = blockIdx.x, N = f.N, C = f.C;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
@@ -516,7 +516,7 @@ __global__ void inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2
 __global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
                                  const float2* __restrict__ ap, const double* __restrict__ pap_parts,
                                  double* __restrict__ rr_parts, CgState* __restrict__ st, int iter) {
-  __shared__ double red[32];
+  __shared__ double red[33];
   const double pap = sum_partials(pap_parts, N, red);
   const double rho = st->rho[iter];
   const bool ok = isfinite(pap) && pap > 0.0;
@@ -548,7 +548,7 @@ __global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restri
 }
 
 __global__ void cg_finish_kernel(int N, const double* __restrict__ rr_parts, CgState* __restrict__ st, int iters) {
-  __shared__ double red[32];
+  __shared__ double red[33];
   const double rho = sum_partials(rr_parts, N, red);
   if (threadIdx.x == 0) {
     st->rho[iters] = rho;

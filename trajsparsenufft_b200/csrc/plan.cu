@@ -605,6 +605,54 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
   }
 }
 
+tsn_status tsn_fft_forward_panel(tsn_plan* plan, const void* x, const void* smaps, void* panel_f16,
+                                 float* panel_scale, tsn_stream_t stream) {
+  try {
+    if (!plan || !x || !panel_f16) fail(TSN_ERR_ARG, "NULL argument");
+    need_views(plan, false, false);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const FftArgs f = fft_args(plan, smaps);
+    CgState* st = plan->state.as<CgState>();
+    const int64_t n = static_cast<int64_t>(plan->N) * plan->N * (smaps ? 1 : plan->C);
+    launch_norm_partials(static_cast<const float2*>(x), n, plan->norm_parts.as<double>(), s);
+    launch_fwd_rows(f, static_cast<const float2*>(x), plan->z1.as<float2>(), 0, nullptr, nullptr,
+                    plan->norm_parts.as<double>(), kNormParts, st, 0, s);
+    launch_fwd_cols(f, plan->z1.as<float2>(), static_cast<__half*>(panel_f16), s);
+    CUDA_OK(cudaGetLastError());
+    if (panel_scale) {
+      float sigma = 0.f;
+      CUDA_OK(cudaMemcpyAsync(&sigma, &st->sigma_x, sizeof(float), cudaMemcpyDeviceToHost, s));
+      CUDA_OK(cudaStreamSynchronize(s));
+      *panel_scale = sigma / static_cast<float>(plan->G);
+    }
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_fft_adjoint_image(tsn_plan* plan, const void* grid_c64, const void* smaps, void* x,
+                                 tsn_stream_t stream) {
+  try {
+    if (!plan || !grid_c64 || !x) fail(TSN_ERR_ARG, "NULL argument");
+    need_views(plan, false, false);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const FftArgs f = fft_args(plan, smaps);
+    CgState* st = plan->state.as<CgState>();
+    // unit sample scale for the plain adjoint epilogue (factor = 1 / sigma_y)
+    const float one = 1.0f;
+    CUDA_OK(cudaMemcpyAsync(&st->sigma_y, &one, sizeof(float), cudaMemcpyHostToDevice, s));
+    launch_inv_cols(f, static_cast<const float2*>(grid_c64), plan->z1.as<float2>(), s);
+    launch_inv_rows(f, plan->z1.as<float2>(), static_cast<float2*>(x), 0, nullptr, nullptr, nullptr, nullptr, st, 0,
+                    1.0f, 0.f, s);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaStreamSynchronize(s));
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
 tsn_status tsn_interp_component(tsn_plan* plan, int32_t view, int32_t component, const void* dense_f16, float* out,
                                 tsn_stream_t stream) {
   try {

@@ -176,6 +176,30 @@ class Plan:
         check(rc)
         return out, hist, status
 
+    def fft_forward_panel(self, x, smaps=None, stream=None):
+        """Forward FFT endpoint: (panel [G*G, 4C] f16 in q1-major rows, panel scale)."""
+        torch = _torch()
+        xp = _dev_ptr(x, torch.complex64, self._image_shape(smaps), "x")
+        sp = None if smaps is None else _dev_ptr(smaps, torch.complex64, (self.coils, self.im_size, self.im_size),
+                                                 "smaps")
+        panel = torch.empty((self.grid_size ** 2, 4 * self.coils), dtype=torch.float16, device=x.device)
+        scale = C.c_float(0.0)
+        check(lib().tsn_fft_forward_panel(self._h, xp, sp, C.c_void_p(panel.data_ptr()), C.byref(scale),
+                                          _stream_handle(stream)))
+        return panel, scale.value
+
+    def fft_adjoint_image(self, grid, smaps=None, out=None, stream=None):
+        """Adjoint FFT endpoint from a grid [G*G, C] c64 in q1-major rows."""
+        torch = _torch()
+        gp = _dev_ptr(grid, torch.complex64, (self.grid_size ** 2, self.coils), "grid")
+        sp = None if smaps is None else _dev_ptr(smaps, torch.complex64, (self.coils, self.im_size, self.im_size),
+                                                 "smaps")
+        if out is None:
+            out = torch.empty(self._image_shape(smaps), dtype=torch.complex64, device=grid.device)
+        xp = _dev_ptr(out, torch.complex64, self._image_shape(smaps), "out")
+        check(lib().tsn_fft_adjoint_image(self._h, gp, sp, xp, _stream_handle(stream)))
+        return out
+
     def interp_component(self, view: str, component: int, dense_f16):
         """Raw out[rows,16] f32 = component(view) @ dense[n_cols,16] (reference.bin contract)."""
         torch = _torch()
