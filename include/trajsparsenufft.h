@@ -204,6 +204,23 @@ tsn_status tsn_fft_forward_panel(tsn_plan* plan, const void* x, const void* smap
 tsn_status tsn_fft_adjoint_image(tsn_plan* plan, const void* grid_c64, const void* smaps, void* x,
                                  tsn_stream_t stream);
 
+/* ---- stage timing (autotuner and roofline reporting) ---------------------------------- */
+enum {
+  TSN_STAGE_FWD_ROWS = 0,   /* forward FFT x-stage (SENSE, deapodization, padding)          */
+  TSN_STAGE_FWD_COLS = 1,   /* forward FFT y-stage -> FP16 hi|res grid panel                 */
+  TSN_STAGE_INTERP_FWD = 2, /* sparse G interpolation -> FP16 hi|res sample panel            */
+  TSN_STAGE_INTERP_ADJ = 3, /* sparse G^H gather -> grid                                     */
+  TSN_STAGE_INV_COLS = 4,   /* inverse FFT first stage                                       */
+  TSN_STAGE_INV_ROWS = 5,   /* inverse FFT second stage + crop + deapod + coil combine      */
+  TSN_STAGE_CG_UPDATE = 6,  /* x, r updates + FP64 partial dots                              */
+  TSN_STAGE_COUNT = 7
+};
+/* Runs one CG-SENSE solve of `iters` iterations to populate the workspaces, then times each
+ * stage of a CG iteration `reps` times in isolation with CUDA events on `stream` and writes
+ * the mean milliseconds per launch to stage_ms[TSN_STAGE_COUNT] (synchronizes). */
+tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, int32_t reps,
+                              double* stage_ms, tsn_stream_t stream);
+
 /* ---- raw interpolation (parity with the reference GPU gate) --------------------------- */
 /* out[rows][16] f32 = component(view) x dense[n_cols][16] f16 for one real/imag component of
  * a plan built from packs: the nufft_gt_spmma_*_f16_f32 contract checked against

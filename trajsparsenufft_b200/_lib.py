@@ -22,12 +22,14 @@ POLICY = {"trajectory": 0, "morton": 1, "overlap": 2, "packing256": 3}
 ILLEGAL = {"split24": 0, "csr_residual": 1}
 VIEW = {"G": 0, "G_T": 1}
 FLAG_REFERENCE_LAYOUT = 1
+STAGES = ("fwd_rows", "fwd_cols", "interp_fwd", "interp_adj", "inv_cols", "inv_rows", "cg_update")
 
 EXPORTED = (
     "tsn_version", "tsn_get_last_error_string", "tsn_plan_desc_default", "tsn_kb_interpolation_csr",
     "tsn_kb_deapodization", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
     "tsn_plan_create_from_pack", "tsn_plan_create_from_trajectory", "tsn_plan_destroy", "tsn_plan_get_info",
     "tsn_forward", "tsn_adjoint", "tsn_cg_sense", "tsn_fft_forward_panel", "tsn_fft_adjoint_image",
+    "tsn_profile_stages",
     "tsn_interp_component",
 )
 
@@ -100,6 +102,7 @@ def lib() -> C.CDLL:
         "tsn_adjoint": (C.c_int, [P, P, P, P, P]),
         "tsn_cg_sense": (C.c_int, [P, P, P, P, F32, F32, I32, P, PF64, C.POINTER(CgStatus), P]),
         "tsn_fft_forward_panel": (C.c_int, [P, P, P, P, PF32, P]),
+        "tsn_profile_stages": (C.c_int, [P, P, P, I32, PF64, P]),
         "tsn_fft_adjoint_image": (C.c_int, [P, P, P, P, P]),
         "tsn_interp_component": (C.c_int, [P, I32, I32, P, P, P]),
     }

@@ -34,41 +34,60 @@ __host__ __device__ constexpr int bitrev(int x, int bits) {
   return bits == 0 ? 0 : (((x & 1) << (bits - 1)) | bitrev(x >> 1, bits - 1));
 }
 
-// In-register DFT of length P (power of two), natural order in and out.
-template <int P, bool INV>
-__device__ __forceinline__ void dft_reg(float2 (&a)[P]) {
-  constexpr int L = ilog2(P);
+// One radix-2 DIT stage of butterfly span LEN, then the next stage (compile-time
+// recursion keeps every register index a constant, so the array never spills to
+// local memory).
+template <int P, bool INV, int LEN>
+struct DitStage {
+  static __device__ __forceinline__ void run(float2 (&a)[P]) {
+    constexpr int HALF = LEN / 2;
 #pragma unroll
-  for (int i = 0; i < P; ++i) {
-    const int j = bitrev(i, L);
-    if (j > i) {
-      const float2 t = a[i];
-      a[i] = a[j];
-      a[j] = t;
-    }
-  }
+    for (int i = 0; i < P; i += LEN) {
 #pragma unroll
-  for (int s = 1; s <= L; ++s) {
-    const int len = 1 << s;
-    const int half = len >> 1;
-#pragma unroll
-    for (int i = 0; i < P; i += len) {
-#pragma unroll
-      for (int j = 0; j < half; ++j) {
+      for (int j = 0; j < HALF; ++j) {
         const float2 u = a[i + j];
-        float2 t = a[i + j + half];
+        float2 t = a[i + j + HALF];
         if (j != 0) {
-          if (4 * j == len) {  // W_len^(len/4) = -i (forward) / +i (inverse)
+          if (4 * j == LEN) {  // W_LEN^(LEN/4) = -i (forward) / +i (inverse)
             t = INV ? make_float2(-t.y, t.x) : make_float2(t.y, -t.x);
           } else {
-            t = cmul(const_twiddle<INV>(j * (1024 / len)), t);
+            t = cmul(const_twiddle<INV>(j * (1024 / LEN)), t);
           }
         }
         a[i + j] = cadd(u, t);
-        a[i + j + half] = csub(u, t);
+        a[i + j + HALF] = csub(u, t);
       }
     }
+    DitStage<P, INV, LEN * 2>::run(a);
   }
+};
+template <int P, bool INV>
+struct DitStage<P, INV, 2 * P> {
+  static __device__ __forceinline__ void run(float2 (&)[P]) {}
+};
+
+template <int P, int I>
+struct BitReverse {
+  static __device__ __forceinline__ void run(float2 (&a)[P]) {
+    constexpr int J = bitrev(I, ilog2(P));
+    if constexpr (J > I) {
+      const float2 t = a[I];
+      a[I] = a[J];
+      a[J] = t;
+    }
+    BitReverse<P, I + 1>::run(a);
+  }
+};
+template <int P>
+struct BitReverse<P, P> {
+  static __device__ __forceinline__ void run(float2 (&)[P]) {}
+};
+
+// In-register DFT of length P (power of two), natural order in and out.
+template <int P, bool INV>
+__device__ __forceinline__ void dft_reg(float2 (&a)[P]) {
+  BitReverse<P, 0>::run(a);
+  DitStage<P, INV, 2>::run(a);
 }
 
 template <int G>

@@ -56,13 +56,17 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   constexpr int CH = BYTES / 16;
   constexpr int NB = ROWH / 8;
   constexpr int NA = SPLIT ? NB / 2 : NB;
+  constexpr int NACC = NCOMP * NA * 4;
+  static_assert(NACC <= kPartialFloats, "partials slot too small");
   extern __shared__ __align__(128) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gidx = blockIdx.x * kInterpWarps + warp;
-  if (gidx >= v.groups) return;
+  const int item_idx = blockIdx.x * kInterpWarps + warp;
+  if (item_idx >= v.n_items) return;
+  const WorkItem item = v.items[item_idx];
+  const int gidx = item.group;
   uint8_t* sb = smem + warp * 2 * 32 * BYTES;
   const uint8_t* pb = reinterpret_cast<const uint8_t*>(panel);
-  const uint32_t t0 = v.group_offsets[gidx], t1 = v.group_offsets[gidx + 1];
+  const uint32_t t0 = item.t0, t1 = item.t1;
   const int g = lane >> 2, t = lane & 3;
 
   float acc[NCOMP][NA][4];
@@ -73,8 +77,10 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[c][a][i] = 0.f;
 
-  auto issue = [&](uint32_t tile, int buf) {
-    const int32_t col = __ldg(reinterpret_cast<const int32_t*>(v.records + static_cast<size_t>(tile) * v.rec_bytes) + lane);
+  auto load_col = [&](uint32_t tile) {
+    return __ldg(reinterpret_cast<const int32_t*>(v.records + static_cast<size_t>(tile) * v.rec_bytes) + lane);
+  };
+  auto issue = [&](int32_t col, int buf) {
     uint8_t* dst = sb + buf * 32 * BYTES;
 #pragma unroll
     for (int i = 0; i < CH; ++i) {
@@ -86,11 +92,17 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
     cp_async_commit();
   };
 
-  if (t0 < t1) issue(t0, 0);
+  // column ids run two tiles ahead of the MMAs, the gather one tile ahead
+  int32_t col_next = 0;
+  if (t0 < t1) issue(load_col(t0), 0);
+  if (t0 + 1 < t1) col_next = load_col(t0 + 1);
   for (uint32_t tile = t0; tile < t1; ++tile) {
     const int buf = (tile - t0) & 1;
     const bool more = tile + 1 < t1;
-    if (more) issue(tile + 1, buf ^ 1);
+    if (more) {
+      issue(col_next, buf ^ 1);
+      if (tile + 2 < t1) col_next = load_col(tile + 2);
+    }
     const uint8_t* rec = v.records + static_cast<size_t>(tile) * v.rec_bytes;
     uint32_t a[NCOMP][4], meta[NCOMP];
 #pragma unroll
@@ -115,6 +127,42 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
       for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
     }
     __syncwarp();
+  }
+
+  if (item.split >= 0) {
+    // split group: publish this chunk, the last chunk to arrive reduces all in order
+    const SplitGroup sg = v.splits[item.split];
+    const int chunk = static_cast<int>((t0 - v.group_offsets[gidx]) / kChunkTiles);
+    float* mine = v.partials + static_cast<size_t>(sg.first_slot + chunk) * kPartialFloats * 32;
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c)
+#pragma unroll
+      for (int a2 = 0; a2 < NA; ++a2)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) mine[((c * NA + a2) * 4 + i) * 32 + lane] = acc[c][a2][i];
+    __threadfence();
+    __syncwarp();
+    int prior = 0;
+    if (lane == 0) prior = atomicAdd(&v.counters[item.split], 1);
+    prior = __shfl_sync(0xFFFFFFFFu, prior, 0);
+    if (prior != sg.nchunks - 1) return;
+    __threadfence();
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c)
+#pragma unroll
+      for (int a2 = 0; a2 < NA; ++a2)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[c][a2][i] = 0.f;
+    for (int k = 0; k < sg.nchunks; ++k) {
+      const float* src = v.partials + static_cast<size_t>(sg.first_slot + k) * kPartialFloats * 32;
+#pragma unroll
+      for (int c = 0; c < NCOMP; ++c)
+#pragma unroll
+        for (int a2 = 0; a2 < NA; ++a2)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[c][a2][i] += __ldcg(src + ((c * NA + a2) * 4 + i) * 32 + lane);
+    }
+    if (lane == 0) v.counters[item.split] = 0;  // ready for the next launch
   }
 
   const int32_t rows[2] = {v.group_rows[gidx * 16 + g], v.group_rows[gidx * 16 + g + 8]};
@@ -178,7 +226,7 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 
 template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
 static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
-  const int blocks = (v.groups + kInterpWarps - 1) / kInterpWarps;
+  const int blocks = (v.n_items + kInterpWarps - 1) / kInterpWarps;
   const size_t smem = static_cast<size_t>(kInterpWarps) * 2 * 32 * ROWH * 2;
   auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -388,19 +436,31 @@ __global__ void split_samples_kernel(const float2* __restrict__ y, const float* 
   __shared__ double red[33];
   const double total = sum_partials(parts, nparts, red);
   const float sigma = pow2_scale(total, static_cast<double>(m) * C, kPanelTarget);
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->sigma_y = sigma;
-  for (int64_t row = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; row < m;
-       row += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->sigma_y = sigma;
+    st->curvature_ok = 1;  // a solve starts here: reset the status words
+    st->finite_ok = 1;
+    st->completed = 0;
+  }
+  const int chunks = C / 4;
+  uint32_t* pu = reinterpret_cast<uint32_t*>(panel);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m * chunks;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = i / chunks;
+    const int q = static_cast<int>(i - row * chunks);
     const float w = sigma * (density ? density[row] : 1.0f);
-    uint32_t* rp = reinterpret_cast<uint32_t*>(panel + row * 4 * C);
-    for (int c = 0; c < C; ++c) {
-      const float2 val = y[static_cast<size_t>(c) * m + row];
-      __half hr, rr, hi, ri;
+    uint32_t hi[4], res[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 val = y[static_cast<size_t>(4 * q + k) * m + row];
+      __half hr, rr, hi_, ri;
       split_hi_res(val.x * w, hr, rr);
-      split_hi_res(val.y * w, hi, ri);
-      rp[c] = pack_half2(hr, hi);
-      rp[C + c] = pack_half2(rr, ri);
+      split_hi_res(val.y * w, hi_, ri);
+      hi[k] = pack_half2(hr, hi_);
+      res[k] = pack_half2(rr, ri);
     }
+    *reinterpret_cast<uint4*>(pu + row * 2 * C + 4 * q) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(pu + row * 2 * C + C + 4 * q) = make_uint4(res[0], res[1], res[2], res[3]);
   }
 }
 
@@ -611,7 +671,7 @@ void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStre
 
 void launch_split_samples(const float2* y, const float* density, int64_t m, int c, __half* panel,
                           const double* partials, int nparts, CgState* st, cudaStream_t s) {
-  const int64_t blocks = std::min<int64_t>((m + 255) / 256, 4 * 148);
+  const int64_t blocks = std::min<int64_t>((m * (c / 4) + 255) / 256, 8 * 148);
   split_samples_kernel<<<static_cast<int>(std::max<int64_t>(blocks, 1)), 256, 0, s>>>(y, density, m, c, panel, partials,
                                                                                         nparts, st);
 }

@@ -30,14 +30,34 @@ struct CgState {
 //   [0,128)            int32 col ids (internal panel row index)
 //   [128+576c, +512)   f16 compressed A of component c, [16][16]
 //   [640+576c, +64)    u32 mma.sp pair metadata of component c, [16]
+// Work item: a run of at most kChunkTiles tiles of one 16-row group. Groups with more
+// tiles are split; their chunks write raw accumulators to `partials` and the warp that
+// arrives last (counter) sums all chunks in chunk order, so results stay deterministic.
+constexpr int kChunkTiles = 8;
+struct WorkItem {
+  int32_t group;
+  uint32_t t0, t1;
+  int32_t split;  // -1: whole group; else split-group id
+};
+struct SplitGroup {
+  int32_t first_slot;
+  int32_t nchunks;
+};
+
 struct InterpView {
   const uint8_t* records = nullptr;
   const uint32_t* group_offsets = nullptr;
   const int32_t* group_rows = nullptr;  // internal row id, -1 pad
+  const WorkItem* items = nullptr;
+  const SplitGroup* splits = nullptr;
+  int32_t* counters = nullptr;          // one per split group, zero between launches
+  float* partials = nullptr;            // [slots][kPartialFloats][32]
   int32_t groups = 0;
+  int32_t n_items = 0;
   int32_t ncomp = 0;
   int32_t rec_bytes = 0;
 };
+constexpr int kPartialFloats = 32;  // >= NCOMP * NA * 4 for every instantiation
 
 enum InterpEpilogue { EPI_SAMPLES = 0, EPI_GRID = 1, EPI_PANEL = 2, EPI_RAW = 3 };
 

@@ -69,7 +69,7 @@ struct HostView {
 };
 
 struct DevView {
-  DeviceBuffer records, offsets, rows;
+  DeviceBuffer records, offsets, rows, items, splits, counters, partials;
   InterpView v;
   int64_t tiles = 0, groups = 0, active_rows = 0, nnz = 0, output_size = 0, n_cols = 0;
   bool present = false;
@@ -133,9 +133,38 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
     const int32_t v = h.group_row_ids[i];
     rows[i] = (v >= 0 && rows_are_cells) ? static_cast<int32_t>(cell_to_internal(v, P->G)) : v;
   }
+  // work items: groups of at most kChunkTiles tiles run whole; longer groups are split into
+  // chunks (scheduled first, they are the long poles) reduced in chunk order
+  std::vector<WorkItem> big, small;
+  std::vector<SplitGroup> splits;
+  int32_t slots = 0;
+  for (int64_t g = 0; g < groups; ++g) {
+    const uint32_t a = h.group_offsets[g], b = h.group_offsets[g + 1];
+    if (b - a <= static_cast<uint32_t>(kChunkTiles)) {
+      small.push_back(WorkItem{static_cast<int32_t>(g), a, b, -1});
+      continue;
+    }
+    const int32_t nch = static_cast<int32_t>((b - a + kChunkTiles - 1) / kChunkTiles);
+    const int32_t sid = static_cast<int32_t>(splits.size());
+    splits.push_back(SplitGroup{slots, nch});
+    slots += nch;
+    for (int32_t k = 0; k < nch; ++k)
+      big.push_back(WorkItem{static_cast<int32_t>(g), a + k * kChunkTiles,
+                             std::min<uint32_t>(b, a + (k + 1) * kChunkTiles), sid});
+  }
+  big.insert(big.end(), small.begin(), small.end());
   d.records.upload(records);
   d.offsets.upload(h.group_offsets);
   d.rows.upload(rows);
+  d.items.upload(big);
+  d.splits.upload(splits);
+  d.counters.upload(std::vector<int32_t>(std::max<size_t>(splits.size(), 1), 0));
+  d.partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kPartialFloats * 32);
+  d.v.items = d.items.as<WorkItem>();
+  d.v.splits = d.splits.as<SplitGroup>();
+  d.v.counters = d.counters.as<int32_t>();
+  d.v.partials = d.partials.as<float>();
+  d.v.n_items = static_cast<int32_t>(big.size());
   d.v.records = d.records.as<uint8_t>();
   d.v.group_offsets = d.offsets.as<uint32_t>();
   d.v.group_rows = d.rows.as<int32_t>();
@@ -599,6 +628,67 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
       if (!host.finite_ok || !std::isfinite(host.rho[iters])) fail(TSN_ERR_NONFINITE, "CG produced non-finite values");
       if (!host.curvature_ok) fail(TSN_ERR_CURVATURE, "CG denominator <= 0 (positive_curvature = 0)");
     }
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, int32_t reps, double* stage_ms,
+                              tsn_stream_t stream) {
+  try {
+    if (!plan || !y || !smaps || !stage_ms || reps <= 0) fail(TSN_ERR_ARG, "invalid argument");
+    need_views(plan, true, true);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    DeviceBuffer xbuf;
+    xbuf.alloc(sizeof(float2) * plan->N * plan->N);
+    enqueue_cg(plan, y, smaps, nullptr, 1e-4f, 1.0f, 2, xbuf.ptr, s);
+    const FftArgs f = fft_args(plan, smaps);
+    CgState* st = plan->state.as<CgState>();
+    float2 *X = xbuf.as<float2>(), *R = plan->r.as<float2>(), *Pv = plan->p.as<float2>(), *AP = plan->ap.as<float2>();
+    double *pap = plan->parts_pap.as<double>(), *rr = plan->parts_rr.as<double>();
+    // iteration index 1 keeps p = r + beta p live; the stages read state written by the solve
+    auto stage = [&](int which) {
+      switch (which) {
+        case TSN_STAGE_FWD_ROWS: launch_fwd_rows(f, nullptr, plan->z1.as<float2>(), 1, Pv, R, rr, plan->N, st, 1, s); break;
+        case TSN_STAGE_FWD_COLS: launch_fwd_cols(f, plan->z1.as<float2>(), plan->panel.as<__half>(), s); break;
+        case TSN_STAGE_INTERP_FWD: {
+          InterpOut o;
+          o.panel = plan->spanel.as<__half>();
+          o.rows = plan->M;
+          o.coils = plan->C;
+          launch_interp(plan->view[TSN_VIEW_G].v, plan->panel.as<__half>(), plan->rowh, true, EPI_PANEL, false, o, s);
+        } break;
+        case TSN_STAGE_INTERP_ADJ: {
+          InterpOut o;
+          o.c64 = plan->grid.as<float2>();
+          o.rows = static_cast<int64_t>(plan->G) * plan->G;
+          o.coils = plan->C;
+          launch_interp(plan->view[TSN_VIEW_GT].v, plan->spanel.as<__half>(), plan->rowh, true, EPI_GRID, true, o, s);
+        } break;
+        case TSN_STAGE_INV_COLS: launch_inv_cols(f, plan->grid.as<float2>(), plan->z1.as<float2>(), s); break;
+        case TSN_STAGE_INV_ROWS:
+          launch_inv_rows(f, plan->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, 1, 1.0f, 1e-4f, s);
+          break;
+        default: launch_cg_update(plan->N, X, R, Pv, AP, pap, rr, st, 1, s); break;
+      }
+    };
+    cudaEvent_t e0, e1;
+    CUDA_OK(cudaEventCreate(&e0));
+    CUDA_OK(cudaEventCreate(&e1));
+    for (int which = 0; which < TSN_STAGE_COUNT; ++which) {
+      stage(which);  // warm
+      CUDA_OK(cudaEventRecord(e0, s));
+      for (int r = 0; r < reps; ++r) stage(which);
+      CUDA_OK(cudaEventRecord(e1, s));
+      CUDA_OK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+      stage_ms[which] = static_cast<double>(ms) / reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CUDA_OK(cudaGetLastError());
     return TSN_OK;
   } catch (const std::exception& e) {
     return guard_status(e);

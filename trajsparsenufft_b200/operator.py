@@ -176,6 +176,15 @@ class Plan:
         check(rc)
         return out, hist, status
 
+    def profile_stages(self, y, smaps, reps=20, stream=None) -> dict:
+        """Mean milliseconds per launch of each CG-iteration stage (CUDA events)."""
+        torch = _torch()
+        yp = _dev_ptr(y, torch.complex64, (self.coils, self.samples), "y")
+        sp = _dev_ptr(smaps, torch.complex64, (self.coils, self.im_size, self.im_size), "smaps")
+        out = np.zeros(len(_lib.STAGES), dtype=np.float64)
+        check(lib().tsn_profile_stages(self._h, yp, sp, int(reps), ptr(out, C.c_double), _stream_handle(stream)))
+        return dict(zip(_lib.STAGES, out.tolist()))
+
     def fft_forward_panel(self, x, smaps=None, stream=None):
         """Forward FFT endpoint: (panel [G*G, 4C] f16 in q1-major rows, panel scale)."""
         torch = _torch()
