@@ -29,7 +29,7 @@ EXPORTED = (
     "tsn_kb_deapodization", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
     "tsn_plan_create_from_pack", "tsn_plan_create_from_trajectory", "tsn_plan_destroy", "tsn_plan_get_info",
     "tsn_forward", "tsn_adjoint", "tsn_cg_sense", "tsn_fft_forward_panel", "tsn_fft_adjoint_image",
-    "tsn_profile_stages",
+    "tsn_profile_stages", "tsn_fft_adjoint_image_static",
     "tsn_interp_component",
 )
 
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
         "tsn_cg_sense": (C.c_int, [P, P, P, P, F32, F32, I32, P, PF64, C.POINTER(CgStatus), P]),
         "tsn_fft_forward_panel": (C.c_int, [P, P, P, P, PF32, P]),
         "tsn_profile_stages": (C.c_int, [P, P, P, I32, PF64, P]),
+        "tsn_fft_adjoint_image_static": (C.c_int, [I32, I32, I32, I32, P, P, P, P, P]),
         "tsn_fft_adjoint_image": (C.c_int, [P, P, P, P, P]),
         "tsn_interp_component": (C.c_int, [P, I32, I32, P, P, P]),
     }
