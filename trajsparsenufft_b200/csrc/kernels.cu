@@ -49,6 +49,14 @@ __device__ __forceinline__ int chunk_swizzle(int ch, int row) {
 
 constexpr int kInterpWarps = 4;
 
+// Per-warp shared-memory ring: stage = tile record (cols, A, meta) + 32 gathered panel rows.
+// Records are fetched kRecAhead tiles ahead, gathers kGatherAhead tiles ahead (the gather
+// needs the record's column ids), so a warp waits only on cp.async groups, never on a
+// register load.
+constexpr int kStages = 5;
+constexpr int kRecAhead = 4;
+constexpr int kGatherAhead = 2;
+
 template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
 __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpView v, const __half* __restrict__ panel,
                                                                          InterpOut o) {
@@ -57,17 +65,21 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   constexpr int NB = ROWH / 8;
   constexpr int NA = SPLIT ? NB / 2 : NB;
   constexpr int NACC = NCOMP * NA * 4;
+  constexpr int REC = 128 + 576 * NCOMP;          // record bytes staged (components used here)
+  constexpr int STAGE = REC + 32 * BYTES;
   static_assert(NACC <= kPartialFloats, "partials slot too small");
+  static_assert(REC % 16 == 0 && STAGE % 16 == 0, "16-byte stages");
   extern __shared__ __align__(128) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item_idx = blockIdx.x * kInterpWarps + warp;
   if (item_idx >= v.n_items) return;
   const WorkItem item = v.items[item_idx];
   const int gidx = item.group;
-  uint8_t* sb = smem + warp * 2 * 32 * BYTES;
+  uint8_t* ring = smem + warp * kStages * STAGE;
   const uint8_t* pb = reinterpret_cast<const uint8_t*>(panel);
   const uint32_t t0 = item.t0, t1 = item.t1;
   const int g = lane >> 2, t = lane & 3;
+  const int ntile = static_cast<int>(t1 - t0);
 
   float acc[NCOMP][NA][4];
 #pragma unroll
@@ -77,47 +89,56 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[c][a][i] = 0.f;
 
-  auto load_col = [&](uint32_t tile) {
-    return __ldg(reinterpret_cast<const int32_t*>(v.records + static_cast<size_t>(tile) * v.rec_bytes) + lane);
+  // record of tile k -> stage k % kStages (component block at v.comp offset 0 / 576)
+  auto issue_record = [&](int k) {
+    if (k >= 0 && k < ntile) {
+      const uint8_t* src = v.records + static_cast<size_t>(t0 + k) * v.rec_bytes;
+      uint8_t* dst = ring + (k % kStages) * STAGE;
+      for (int c = lane; c < REC / 16; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
+    }
+    cp_async_commit();  // empty groups keep the group arithmetic uniform
   };
-  auto issue = [&](int32_t col, int buf) {
-    uint8_t* dst = sb + buf * 32 * BYTES;
+  auto issue_gather = [&](int k) {
+    if (k >= 0 && k < ntile) {
+      uint8_t* st = ring + (k % kStages) * STAGE;
+      const int32_t col = reinterpret_cast<const int32_t*>(st)[lane];
+      uint8_t* dst = st + REC;
 #pragma unroll
-    for (int i = 0; i < CH; ++i) {
-      const int ci = lane + 32 * i;
-      const int row = ci / CH, ch = ci % CH;
-      const int src = __shfl_sync(0xFFFFFFFFu, col, row);
-      cp_async16(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16, pb + static_cast<size_t>(src) * BYTES + ch * 16);
+      for (int i = 0; i < CH; ++i) {
+        const int ci = lane + 32 * i;
+        const int row = ci / CH, ch = ci % CH;
+        const int src = __shfl_sync(0xFFFFFFFFu, col, row);
+        cp_async16(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16, pb + static_cast<size_t>(src) * BYTES + ch * 16);
+      }
     }
     cp_async_commit();
   };
 
-  // column ids run two tiles ahead of the MMAs, the gather one tile ahead
-  int32_t col_next = 0;
-  if (t0 < t1) issue(load_col(t0), 0);
-  if (t0 + 1 < t1) col_next = load_col(t0 + 1);
-  for (uint32_t tile = t0; tile < t1; ++tile) {
-    const int buf = (tile - t0) & 1;
-    const bool more = tile + 1 < t1;
-    if (more) {
-      issue(col_next, buf ^ 1);
-      if (tile + 2 < t1) col_next = load_col(tile + 2);
-    }
-    const uint8_t* rec = v.records + static_cast<size_t>(tile) * v.rec_bytes;
+  // Uniform iterations k = -kRecAhead .. ntile-1, two commit groups each (empty when out of
+  // range).  Newest-first the pending groups before "wait<4>" are
+  //   [rec(k+4), gat(k+1), rec(k+3), gat(k), rec(k+2), ...]   -> rec(k+2) has landed
+  // and after issuing gat(k+2)
+  //   [gat(k+2), rec(k+4), gat(k+1), rec(k+3), gat(k), ...]   -> gat(k) has landed.
+  static_assert(kRecAhead == 4 && kGatherAhead == 2 && kStages == kRecAhead + 1, "group arithmetic");
+  for (int k = -kRecAhead; k < ntile; ++k) {
+    issue_record(k + kRecAhead);
+    cp_async_wait<4>();
+    __syncwarp();
+    issue_gather(k + kGatherAhead);
+    cp_async_wait<4>();
+    __syncwarp();
+    if (k < 0) continue;
+    uint8_t* st = ring + (k % kStages) * STAGE;
     uint32_t a[NCOMP][4], meta[NCOMP];
 #pragma unroll
     for (int c = 0; c < NCOMP; ++c) {
-      const uint32_t* A = reinterpret_cast<const uint32_t*>(rec + 128 + 576 * c);
-      a[c][0] = __ldg(A + g * 8 + t);
-      a[c][1] = __ldg(A + (g + 8) * 8 + t);
-      a[c][2] = __ldg(A + g * 8 + 4 + t);
-      a[c][3] = __ldg(A + (g + 8) * 8 + 4 + t);
-      meta[c] = __ldg(reinterpret_cast<const uint32_t*>(rec + 640 + 576 * c) + g * 2 + (t & 1));
+      // A rows of 32 B; the 16-B halves of row r are stored swapped when (r >> 2) & 1
+      const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
+      const int half = lane >> 4;
+      ldmatrix_x4(a[c], st + 128 + 576 * c + r * 32 + ((half ^ ((r >> 2) & 1)) * 16));
+      meta[c] = reinterpret_cast<const uint32_t*>(st + 640 + 576 * c)[g * 2 + (t & 1)];
     }
-    if (more) cp_async_wait<1>();
-    else cp_async_wait<0>();
-    __syncwarp();
-    const uint8_t* B = sb + buf * 32 * BYTES;
+    const uint8_t* B = st + REC;
 #pragma unroll
     for (int nb = 0; nb < NB; ++nb) {
       uint32_t b[4];
@@ -126,8 +147,9 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 #pragma unroll
       for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
     }
-    __syncwarp();
+    __syncwarp();  // stage k is reused by record(k + kStages) next iteration
   }
+  cp_async_wait<0>();
 
   if (item.split >= 0) {
     // split group: publish this chunk, the last chunk to arrive reduces all in order
@@ -227,7 +249,7 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
 static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
   const int blocks = (v.n_items + kInterpWarps - 1) / kInterpWarps;
-  const size_t smem = static_cast<size_t>(kInterpWarps) * 2 * 32 * ROWH * 2;
+  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (128 + 576 * NCOMP + 32 * ROWH * 2);
   auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (blocks > 0) k<<<blocks, kInterpWarps * 32, smem, s>>>(v, panel, o);
@@ -300,132 +322,185 @@ __device__ __forceinline__ void load_twiddles(float2* tw_s, const float2* tw, in
   for (int i = threadIdx.x; i < G; i += blockDim.x) tw_s[i] = tw[i];
 }
 
+// Copy `bytes` (multiple of 16) from global to shared with 16-byte cp.async, all threads.
+__device__ __forceinline__ void cp_async_bytes(void* dst, const void* src, int bytes) {
+  uint8_t* d = static_cast<uint8_t*>(dst);
+  const uint8_t* q = static_cast<const uint8_t*>(src);
+  for (int i = threadIdx.x * 16; i < bytes; i += blockDim.x * 16) cp_async16(d + i, q + i);
+}
+
+// The four FFT stages are persistent CTAs (one warp per coil) walking their items with a
+// double-buffered cp.async input slab: item i+1 streams in while item i is transformed.
+
 // Forward rows (x-stage). Image row i0 -> z1[q1][i0][c] for all q1. Fuses the SENSE
 // multiply, deapodization, power-of-two panel scaling, zero-padding and (CG) p = r + beta p.
+// Input slab per row: [row0 N][row1 N][maps C*N] float2 + [scaling N] float
+//   mode 0 with smaps:  row0 = x row, maps = S_c rows      (row1 unused)
+//   mode 0 without:     maps = coil-image rows
+//   mode 1 (CG):        row0 = r row, row1 = p row, maps = S_c rows
 // Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844).
 template <int G>
-__global__ void fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1, int mode,
-                                float2* __restrict__ p, const float2* __restrict__ r, const double* __restrict__ parts,
-                                int nparts, CgState* __restrict__ st, int iter) {
+__global__ void __launch_bounds__(512) fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1,
+                                                       int mode, float2* __restrict__ p, const float2* __restrict__ r,
+                                                       const double* __restrict__ parts, int nparts,
+                                                       CgState* __restrict__ st, int iter) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
+  const int N = f.N, C = f.C;
+  const int in_f2 = (2 + C) * N;                         // float2 per slab (+ N floats of scaling)
+  const int in_bytes = in_f2 * 8 + N * 4;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* row_s = tw_s + G;                        // [N]
-  float2* out_s = row_s + f.N;                     // [G][C]
-  float2* scr = out_s + G * f.C;                   // [C][SCR]
+  uint8_t* inb = reinterpret_cast<uint8_t*>(tw_s + G);   // [2][in_bytes]
+  float2* out_s = reinterpret_cast<float2*>(inb + 2 * in_bytes);  // [G][C]
+  float2* scr = out_s + G * C;                           // [C][SCR]
   __shared__ double red[33];
-  const int i0 = blockIdx.x, N = f.N, C = f.C;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
   const double total = sum_partials(parts, nparts, red);
   float sigma;
+  double beta = 0.0;
   if (mode == 0) {
-    const double count = static_cast<double>(N) * N * (f.smaps ? 1 : C);
-    sigma = pow2_scale(total, count, kPanelTarget);
-    if (i0 == 0 && threadIdx.x == 0) st->sigma_x = sigma;
-    if (f.smaps) {
-      for (int i = threadIdx.x; i < N; i += blockDim.x) row_s[i] = x[static_cast<size_t>(i0) * N + i];
-    }
+    sigma = pow2_scale(total, static_cast<double>(N) * N * (f.smaps ? 1 : C), kPanelTarget);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->sigma_x = sigma;
   } else {
-    const double rho = total;
-    sigma = pow2_scale(rho, static_cast<double>(N) * N, kPanelTarget);
-    const double beta = iter == 0 ? 0.0 : rho / fmax(st->rho[iter - 1], 1e-30);
-    if (i0 == 0 && threadIdx.x == 0) {
-      st->rho[iter] = rho;
+    sigma = pow2_scale(total, static_cast<double>(N) * N, kPanelTarget);
+    beta = iter == 0 ? 0.0 : total / fmax(st->rho[iter - 1], 1e-30);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->rho[iter] = total;
       st->beta[iter] = beta;
       st->sigma[iter] = sigma;
     }
-    const float bf = static_cast<float>(beta);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-      const size_t idx = static_cast<size_t>(i0) * N + i;
-      const float2 rv = r[idx];
-      float2 pv = rv;
-      if (iter > 0) {
-        const float2 po = p[idx];
-        pv = make_float2(rv.x + bf * po.x, rv.y + bf * po.y);
-      }
-      p[idx] = pv;
-      row_s[i] = pv;
-    }
   }
-  __syncthreads();
+  const float bf = static_cast<float>(beta);
   const float scl = sigma / static_cast<float>(G);
-  if (warp < C) {
-    const int c = warp;
-    float2 v[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-      const int n = lane + 32 * j;
-      int i1 = n + f.shift;
-      if (i1 >= G) i1 -= G;
-      float2 val = make_float2(0.f, 0.f);
-      if (i1 < N) {
-        const size_t pix = static_cast<size_t>(i0) * N + i1;
-        const float d = f.scaling[pix] * scl;
-        if (f.smaps) {
-          val = cscale(cmul(row_s[i1], f.smaps[static_cast<size_t>(c) * N * N + pix]), d);
-        } else {
-          val = cscale(x[static_cast<size_t>(c) * N * N + pix], d);
-        }
-      }
-      v[j] = val;
+  auto prefetch = [&](int i0, int buf) {
+    uint8_t* dst = inb + buf * in_bytes;
+    float2* row0 = reinterpret_cast<float2*>(dst);
+    float2* row1 = row0 + N;
+    float2* maps = row1 + N;
+    const size_t off = static_cast<size_t>(i0) * N;
+    if (mode == 1) {
+      cp_async_bytes(row0, r + off, N * 8);
+      if (iter > 0) cp_async_bytes(row1, p + off, N * 8);
+    } else if (f.smaps) {
+      cp_async_bytes(row0, x + off, N * 8);
     }
-    warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
+    const float2* msrc = f.smaps ? f.smaps : x;
+    for (int c = 0; c < C; ++c) cp_async_bytes(maps + c * N, msrc + static_cast<size_t>(c) * N * N + off, N * 8);
+    cp_async_bytes(dst + in_f2 * 8, f.scaling + off, N * 4);
+    cp_async_commit();
+  };
+  int buf = 0;
+  if (blockIdx.x < N) prefetch(blockIdx.x, 0);
+  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x, buf ^= 1) {
+    const int next = i0 + gridDim.x;
+    if (next < N) {
+      prefetch(next, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    uint8_t* in = inb + buf * in_bytes;
+    float2* row0 = reinterpret_cast<float2*>(in);
+    const float2* row1 = row0 + N;
+    const float2* maps = row1 + N;
+    const float* srow = reinterpret_cast<const float*>(in + in_f2 * 8);
+    if (mode == 1) {  // p = r + beta p (p = r at iteration 0); row0 becomes p
+      for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        float2 pv = row0[i];
+        if (iter > 0) {
+          const float2 po = row1[i];
+          pv = make_float2(pv.x + bf * po.x, pv.y + bf * po.y);
+        }
+        row0[i] = pv;
+        p[static_cast<size_t>(i0) * N + i] = pv;
+      }
+      __syncthreads();
+    }
+    if (warp < C) {
+      const int c = warp;
+      float2 v[P];
 #pragma unroll
-    for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * C + c] = v[m];
-  }
-  __syncthreads();
-  // z1[q1][i0][c]: C contiguous values per q1
-  for (int e = threadIdx.x; e < G * C; e += blockDim.x) {
-    const int q1 = e / C, c = e - q1 * C;
-    z1[(static_cast<size_t>(q1) * N + i0) * C + c] = out_s[e];
+      for (int j = 0; j < P; ++j) {
+        const int n = lane + 32 * j;
+        int i1 = n + f.shift;
+        if (i1 >= G) i1 -= G;
+        float2 val = make_float2(0.f, 0.f);
+        if (i1 < N) {
+          const float d = srow[i1] * scl;
+          val = (f.smaps || mode == 1) ? cscale(cmul(row0[i1], maps[c * N + i1]), d) : cscale(maps[c * N + i1], d);
+        }
+        v[j] = val;
+      }
+      warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
+#pragma unroll
+      for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * C + c] = v[m];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * C; e += blockDim.x) {
+      const int q1 = e / C, c = e - q1 * C;
+      z1[(static_cast<size_t>(q1) * N + i0) * C + c] = out_s[e];
+    }
   }
 }
 
 // Forward columns (y-stage): z1[q1][*][c] -> panel rows q1*G + q0, FP16 hi | res.
 // Reference: fft512_allcoils1_shared16_to_n16 (nufft_custom_fft_forward_bench.cu:538-747).
 template <int G>
-__global__ void fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1, __half* __restrict__ panel) {
+__global__ void __launch_bounds__(512) fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1,
+                                                       __half* __restrict__ panel) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
+  const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* in_s = tw_s + G;               // [N][C]
-  float2* scr = in_s + f.N * f.C;        // [C][SCR]
-  uint32_t* out_s = reinterpret_cast<uint32_t*>(scr + f.C * FftSmem<G>::SCR);  // [G][2C] half2
-  const int q1 = blockIdx.x, N = f.N, C = f.C;
+  float2* inb = tw_s + G;                              // [2][N*C]
+  float2* scr = inb + 2 * N * C;                       // [C][SCR]
+  uint32_t* out_s = reinterpret_cast<uint32_t*>(scr + C * FftSmem<G>::SCR);  // [G][2C] half2
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
-  {
-    const float4* src = reinterpret_cast<const float4*>(z1 + static_cast<size_t>(q1) * N * C);
-    float4* dst = reinterpret_cast<float4*>(in_s);
-    for (int i = threadIdx.x; i < N * C / 2; i += blockDim.x) dst[i] = src[i];
-  }
-  __syncthreads();
-  if (warp < C) {
-    const int c = warp;
-    float2 v[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-      const int n = lane + 32 * j;
-      int i0 = n + f.shift;
-      if (i0 >= G) i0 -= G;
-      v[j] = i0 < N ? in_s[i0 * C + c] : make_float2(0.f, 0.f);
+  auto prefetch = [&](int q1, int buf) {
+    cp_async_bytes(inb + buf * N * C, z1 + static_cast<size_t>(q1) * N * C, N * C * 8);
+    cp_async_commit();
+  };
+  int buf = 0;
+  if (blockIdx.x < G) prefetch(blockIdx.x, 0);
+  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, buf ^= 1) {
+    const int next = q1 + gridDim.x;
+    if (next < G) {
+      prefetch(next, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
-    warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();
+    const float2* in_s = inb + buf * N * C;
+    if (warp < C) {
+      const int c = warp;
+      float2 v[P];
 #pragma unroll
-    for (int m = 0; m < P; ++m) {
-      const int q0 = warp_fft_out_index<G>(m);
-      __half hr, rr, hi, ri;
-      split_hi_res(v[m].x, hr, rr);
-      split_hi_res(v[m].y, hi, ri);
-      out_s[q0 * 2 * C + c] = pack_half2(hr, hi);
-      out_s[q0 * 2 * C + C + c] = pack_half2(rr, ri);
+      for (int j = 0; j < P; ++j) {
+        const int n = lane + 32 * j;
+        int i0 = n + f.shift;
+        if (i0 >= G) i0 -= G;
+        v[j] = i0 < N ? in_s[i0 * C + c] : make_float2(0.f, 0.f);
+      }
+      warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        const int q0 = warp_fft_out_index<G>(m);
+        __half hr, rr, hi, ri;
+        split_hi_res(v[m].x, hr, rr);
+        split_hi_res(v[m].y, hi, ri);
+        out_s[q0 * 2 * C + c] = pack_half2(hr, hi);
+        out_s[q0 * 2 * C + C + c] = pack_half2(rr, ri);
+      }
     }
+    __syncthreads();
+    const int4* src = reinterpret_cast<const int4*>(out_s);
+    int4* dst = reinterpret_cast<int4*>(panel + static_cast<size_t>(q1) * G * 4 * C);
+    for (int i = threadIdx.x; i < G * C / 2; i += blockDim.x) dst[i] = src[i];
   }
-  __syncthreads();
-  const int4* src = reinterpret_cast<const int4*>(out_s);
-  int4* dst = reinterpret_cast<int4*>(panel + static_cast<size_t>(q1) * G * 4 * C);
-  for (int i = threadIdx.x; i < G * C / 2; i += blockDim.x) dst[i] = src[i];
 }
 
 // Measurement / adjoint input [C][M] -> sample panel [M][4C] with sigma_y and density.
@@ -467,109 +542,141 @@ __global__ void split_samples_kernel(const float2* __restrict__ y, const float* 
 // Inverse columns: grid rows q1*G + [0,G) (all coils) -> w1[q1][i0][c], i0 < N (crop).
 // Reference: ifft512_rows8_regular_transposed (nufft_custom_fft_forward_bench.cu:1463-1515).
 template <int G>
-__global__ void inv_cols_kernel(FftArgs f, const float2* __restrict__ grid, float2* __restrict__ w1) {
+__global__ void __launch_bounds__(512) inv_cols_kernel(FftArgs f, const float2* __restrict__ grid,
+                                                       float2* __restrict__ w1) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
+  const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* in_s = tw_s + G;               // [G][C]
-  float2* out_s = in_s + G * f.C;        // [N][C]
-  float2* scr = out_s + f.N * f.C;       // [C][SCR]
-  const int q1 = blockIdx.x, N = f.N, C = f.C;
+  float2* inb = tw_s + G;                // [2][G*C]
+  float2* out_s = inb + 2 * G * C;       // [N][C]
+  float2* scr = out_s + N * C;           // [C][SCR]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
-  {
-    const float4* src = reinterpret_cast<const float4*>(grid + static_cast<size_t>(q1) * G * C);
-    float4* dst = reinterpret_cast<float4*>(in_s);
-    for (int i = threadIdx.x; i < G * C / 2; i += blockDim.x) dst[i] = src[i];
-  }
-  __syncthreads();
-  if (warp < C) {
-    const int c = warp;
-    float2 v[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) v[j] = in_s[(lane + 32 * j) * C + c];
-    warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-      int i0 = warp_fft_out_index<G>(m) + f.shift;
-      if (i0 >= G) i0 -= G;
-      if (i0 < N) out_s[i0 * C + c] = v[m];
+  auto prefetch = [&](int q1, int buf) {
+    cp_async_bytes(inb + buf * G * C, grid + static_cast<size_t>(q1) * G * C, G * C * 8);
+    cp_async_commit();
+  };
+  int buf = 0;
+  if (blockIdx.x < G) prefetch(blockIdx.x, 0);
+  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, buf ^= 1) {
+    const int next = q1 + gridDim.x;
+    if (next < G) {
+      prefetch(next, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
+    __syncthreads();
+    const float2* in_s = inb + buf * G * C;
+    if (warp < C) {
+      const int c = warp;
+      float2 v[P];
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = in_s[(lane + 32 * j) * C + c];
+      warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        int i0 = warp_fft_out_index<G>(m) + f.shift;
+        if (i0 >= G) i0 -= G;
+        if (i0 < N) out_s[i0 * C + c] = v[m];
+      }
+    }
+    __syncthreads();
+    const float4* src = reinterpret_cast<const float4*>(out_s);
+    float4* dst = reinterpret_cast<float4*>(w1 + static_cast<size_t>(q1) * N * C);
+    for (int i = threadIdx.x; i < N * C / 2; i += blockDim.x) dst[i] = src[i];
   }
-  __syncthreads();
-  const float4* src = reinterpret_cast<const float4*>(out_s);
-  float4* dst = reinterpret_cast<float4*>(w1 + static_cast<size_t>(q1) * N * C);
-  for (int i = threadIdx.x; i < N * C / 2; i += blockDim.x) dst[i] = src[i];
 }
 
 // Inverse rows + crop + deapodization + SENSE coil combine (+ CG epilogues).
 // Reference: ifft512_rows8_regular_crop_scale (nufft_custom_fft_forward_bench.cu:1517-1552)
 // followed by sense_combine_scaled (nufft_fp16x2_cg_bench.cu:27-54).
 template <int G>
-__global__ void inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2* __restrict__ out, int mode,
-                                float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
-                                double* __restrict__ parts, CgState* __restrict__ st, int iter, float inv_scale2,
-                                float lambda_scaled) {
+__global__ void __launch_bounds__(512) inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2* __restrict__ out,
+                                                       int mode, float2* __restrict__ x, float2* __restrict__ r,
+                                                       const float2* __restrict__ p, double* __restrict__ parts,
+                                                       CgState* __restrict__ st, int iter, float inv_scale2,
+                                                       float lambda_scaled) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
+  const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* in_s = tw_s + G;               // [G][C]
-  float2* img_s = in_s + G * f.C;        // [C][N]
-  float2* scr = img_s + f.N * f.C;       // [C][SCR]
+  float2* inb = tw_s + G;                // [2][G*C]
+  float2* img_s = inb + 2 * G * C;       // [C][N]
+  float2* scr = img_s + N * C;           // [C][SCR]
   __shared__ double red[33];
-  const int i0 = blockIdx.x, N = f.N, C = f.C;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
-  for (int e = threadIdx.x; e < G * C; e += blockDim.x) {
-    const int q1 = e / C, c = e - q1 * C;
-    in_s[e] = w1[(static_cast<size_t>(q1) * N + i0) * C + c];
-  }
-  __syncthreads();
-  if (warp < C) {
-    const int c = warp;
-    float2 v[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) v[j] = in_s[(lane + 32 * j) * C + c];
-    warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-      int i1 = warp_fft_out_index<G>(m) + f.shift;
-      if (i1 >= G) i1 -= G;
-      if (i1 < N) img_s[c * N + i1] = v[m];
-    }
-  }
-  __syncthreads();
   float factor;
   if (mode == 2) factor = static_cast<float>(G) / st->sigma[iter] * inv_scale2;
   else factor = inv_scale2 / st->sigma_y;
-  double dot = 0.0;
-  for (int i1 = threadIdx.x; i1 < N; i1 += blockDim.x) {
-    const size_t pix = static_cast<size_t>(i0) * N + i1;
-    const float d = f.scaling[pix] * factor;
-    if (!f.smaps) {  // coil images out [C][N][N]
-      for (int c = 0; c < C; ++c) out[static_cast<size_t>(c) * N * N + pix] = cscale(img_s[c * N + i1], d);
-      continue;
+  auto prefetch = [&](int i0, int buf) {
+    float2* dst = inb + buf * G * C;
+    // G runs of C complex values (8C bytes each, 16-byte aligned for even C)
+    const int chunks_per_run = C / 2;
+    for (int e = threadIdx.x; e < G * chunks_per_run; e += blockDim.x) {
+      const int q1 = e / chunks_per_run, k = e - q1 * chunks_per_run;
+      cp_async16(dst + q1 * C + 2 * k, w1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * k);
     }
-    float2 acc = make_float2(0.f, 0.f);
-    for (int c = 0; c < C; ++c) acc = cadd(acc, cmulc(img_s[c * N + i1], f.smaps[static_cast<size_t>(c) * N * N + pix]));
-    acc = cscale(acc, d);
-    if (mode == 0) {
-      out[pix] = acc;
-    } else if (mode == 1) {
-      r[pix] = acc;
-      x[pix] = make_float2(0.f, 0.f);
-      dot += static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y;
+    cp_async_commit();
+  };
+  int buf = 0;
+  if (blockIdx.x < N) prefetch(blockIdx.x, 0);
+  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x, buf ^= 1) {
+    const int next = i0 + gridDim.x;
+    if (next < N) {
+      prefetch(next, buf ^ 1);
+      cp_async_wait<1>();
     } else {
-      const float2 pv = p[pix];
-      acc.x += lambda_scaled * pv.x;
-      acc.y += lambda_scaled * pv.y;
-      out[pix] = acc;
-      dot += static_cast<double>(pv.x) * acc.x + static_cast<double>(pv.y) * acc.y;
+      cp_async_wait<0>();
     }
-  }
-  if (mode != 0) {
-    const double t = block_sum(dot, red);
-    if (threadIdx.x == 0) parts[i0] = t;
+    __syncthreads();
+    const float2* in_s = inb + buf * G * C;
+    if (warp < C) {
+      const int c = warp;
+      float2 v[P];
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = in_s[(lane + 32 * j) * C + c];
+      warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        int i1 = warp_fft_out_index<G>(m) + f.shift;
+        if (i1 >= G) i1 -= G;
+        if (i1 < N) img_s[c * N + i1] = v[m];
+      }
+    }
+    __syncthreads();
+    double dot = 0.0;
+    for (int i1 = threadIdx.x; i1 < N; i1 += blockDim.x) {
+      const size_t pix = static_cast<size_t>(i0) * N + i1;
+      const float d = f.scaling[pix] * factor;
+      if (!f.smaps) {  // coil images out [C][N][N]
+        for (int c = 0; c < C; ++c) out[static_cast<size_t>(c) * N * N + pix] = cscale(img_s[c * N + i1], d);
+        continue;
+      }
+      float2 acc = make_float2(0.f, 0.f);
+      for (int c = 0; c < C; ++c)
+        acc = cadd(acc, cmulc(img_s[c * N + i1], f.smaps[static_cast<size_t>(c) * N * N + pix]));
+      acc = cscale(acc, d);
+      if (mode == 0) {
+        out[pix] = acc;
+      } else if (mode == 1) {
+        r[pix] = acc;
+        x[pix] = make_float2(0.f, 0.f);
+        dot += static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y;
+      } else {
+        const float2 pv = p[pix];
+        acc.x += lambda_scaled * pv.x;
+        acc.y += lambda_scaled * pv.y;
+        out[pix] = acc;
+        dot += static_cast<double>(pv.x) * acc.x + static_cast<double>(pv.y) * acc.y;
+      }
+    }
+    if (mode != 0) {
+      const double t = block_sum(dot, red);
+      if (threadIdx.x == 0) parts[i0] = t;
+    }
   }
 }
 
@@ -621,16 +728,17 @@ __global__ void cg_finish_kernel(int N, const double* __restrict__ rr_parts, CgS
 // ------------------------------------------------------------------------------------------
 template <int G>
 static size_t fwd_rows_smem(const FftArgs& f) {
-  return sizeof(float2) * (G + f.N + static_cast<size_t>(G) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR);
+  const size_t in_bytes = static_cast<size_t>(2 + f.C) * f.N * 8 + static_cast<size_t>(f.N) * 4;
+  return sizeof(float2) * G + 2 * in_bytes + sizeof(float2) * (static_cast<size_t>(G) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR);
 }
 template <int G>
 static size_t fwd_cols_smem(const FftArgs& f) {
-  return sizeof(float2) * (G + static_cast<size_t>(f.N) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR) +
+  return sizeof(float2) * (G + 2 * static_cast<size_t>(f.N) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR) +
          sizeof(uint32_t) * static_cast<size_t>(G) * 2 * f.C;
 }
 template <int G>
 static size_t inv_cols_smem(const FftArgs& f) {
-  return sizeof(float2) * (G + static_cast<size_t>(G) * f.C + static_cast<size_t>(f.N) * f.C +
+  return sizeof(float2) * (G + 2 * static_cast<size_t>(G) * f.C + static_cast<size_t>(f.N) * f.C +
                            static_cast<size_t>(f.C) * FftSmem<G>::SCR);
 }
 template <int G>
@@ -641,6 +749,26 @@ static size_t inv_rows_smem(const FftArgs& f) {
 template <class K>
 static void ensure_smem(K k, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// persistent grid: resident CTAs per SM x SMs, capped by the item count
+template <class K>
+static int persistent_grid(K k, int threads, size_t smem, int items) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+  const int grid = std::max(1, per_sm) * sm_count();
+  return std::max(1, std::min(grid, items));
 }
 
 #define TSN_G_SWITCH(G_, ...)                                  \
@@ -657,7 +785,8 @@ void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, fl
   TSN_G_SWITCH(f.G, {
     const size_t sm = fwd_rows_smem<GG>(f);
     ensure_smem(fwd_rows_kernel<GG>, sm);
-    fwd_rows_kernel<GG><<<f.N, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
+    const int grid = persistent_grid(fwd_rows_kernel<GG>, 32 * f.C, sm, f.N);
+    fwd_rows_kernel<GG><<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
   });
 }
 
@@ -665,7 +794,8 @@ void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStre
   TSN_G_SWITCH(f.G, {
     const size_t sm = fwd_cols_smem<GG>(f);
     ensure_smem(fwd_cols_kernel<GG>, sm);
-    fwd_cols_kernel<GG><<<f.G, 32 * f.C, sm, s>>>(f, z1, panel);
+    const int grid = persistent_grid(fwd_cols_kernel<GG>, 32 * f.C, sm, f.G);
+    fwd_cols_kernel<GG><<<grid, 32 * f.C, sm, s>>>(f, z1, panel);
   });
 }
 
@@ -680,7 +810,8 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
   TSN_G_SWITCH(f.G, {
     const size_t sm = inv_cols_smem<GG>(f);
     ensure_smem(inv_cols_kernel<GG>, sm);
-    inv_cols_kernel<GG><<<f.G, 32 * f.C, sm, s>>>(f, grid, w1);
+    const int g = persistent_grid(inv_cols_kernel<GG>, 32 * f.C, sm, f.G);
+    inv_cols_kernel<GG><<<g, 32 * f.C, sm, s>>>(f, grid, w1);
   });
 }
 
@@ -689,8 +820,9 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
   TSN_G_SWITCH(f.G, {
     const size_t sm = inv_rows_smem<GG>(f);
     ensure_smem(inv_rows_kernel<GG>, sm);
-    inv_rows_kernel<GG><<<f.N, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2,
-                                                   lambda_scaled);
+    const int g = persistent_grid(inv_rows_kernel<GG>, 32 * f.C, sm, f.N);
+    inv_rows_kernel<GG><<<g, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2,
+                                                 lambda_scaled);
   });
 }
 

@@ -124,7 +124,12 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
     }
     std::memcpy(r, cols, sizeof cols);
     for (int c = 0; c < ncomp; ++c) {
-      std::memcpy(r + 128 + 576 * c, &h.a[c][t * 256], 512);
+      // A: 16 rows of 32 B; the two 16-B halves of row r are swapped when (r >> 2) & 1 so
+      // ldmatrix reads 8 rows of one half without shared-memory bank conflicts
+      for (int row = 0; row < 16; ++row)
+        for (int half = 0; half < 2; ++half)
+          std::memcpy(r + 128 + 576 * c + row * 32 + ((half ^ ((row >> 2) & 1)) * 16),
+                      &h.a[c][t * 256 + row * 16 + half * 8], 16);
       std::memcpy(r + 640 + 576 * c, &h.meta[c][t * 16], 64);
     }
   }
