@@ -52,108 +52,21 @@ constexpr int kInterpWarps = 4;
 // Per-warp shared-memory ring: stage = tile record (cols, A, meta) + 32 gathered panel rows.
 // Records are fetched kRecAhead tiles ahead, gathers kGatherAhead tiles ahead (the gather
 // needs the record's column ids), so a warp waits only on cp.async groups, never on a
-// register load.
+// register load.  Warps are persistent: each streams a contiguous, tile-balanced run of
+// work items and the pipeline runs across item boundaries.
 constexpr int kStages = 5;
 constexpr int kRecAhead = 4;
 constexpr int kGatherAhead = 2;
 
-template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
-__global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpView v, const __half* __restrict__ panel,
-                                                                         InterpOut o) {
-  constexpr int BYTES = ROWH * 2;
-  constexpr int CH = BYTES / 16;
-  constexpr int NB = ROWH / 8;
-  constexpr int NA = SPLIT ? NB / 2 : NB;
-  constexpr int NACC = NCOMP * NA * 4;
-  constexpr int REC = 128 + 576 * NCOMP;          // record bytes staged (components used here)
-  constexpr int STAGE = REC + 32 * BYTES;
-  static_assert(NACC <= kPartialFloats, "partials slot too small");
-  static_assert(REC % 16 == 0 && STAGE % 16 == 0, "16-byte stages");
-  extern __shared__ __align__(128) uint8_t smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int item_idx = blockIdx.x * kInterpWarps + warp;
-  if (item_idx >= v.n_items) return;
-  const WorkItem item = v.items[item_idx];
-  const int gidx = item.group;
-  uint8_t* ring = smem + warp * kStages * STAGE;
-  const uint8_t* pb = reinterpret_cast<const uint8_t*>(panel);
-  const uint32_t t0 = item.t0, t1 = item.t1;
+// Writes one finished item: split chunks publish their accumulators and the last chunk of
+// the group reduces all chunks in chunk order; whole groups and finishing chunks apply the
+// epilogue.
+template <int ROWH, int NCOMP, int NA, int EPI, bool CONJ>
+__device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], const InterpView& v,
+                                                   const InterpOut& o, int gidx, int split, uint32_t t0, int lane) {
   const int g = lane >> 2, t = lane & 3;
-  const int ntile = static_cast<int>(t1 - t0);
-
-  float acc[NCOMP][NA][4];
-#pragma unroll
-  for (int c = 0; c < NCOMP; ++c)
-#pragma unroll
-    for (int a = 0; a < NA; ++a)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) acc[c][a][i] = 0.f;
-
-  // record of tile k -> stage k % kStages (component block at v.comp offset 0 / 576)
-  auto issue_record = [&](int k) {
-    if (k >= 0 && k < ntile) {
-      const uint8_t* src = v.records + static_cast<size_t>(t0 + k) * v.rec_bytes;
-      uint8_t* dst = ring + (k % kStages) * STAGE;
-      for (int c = lane; c < REC / 16; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
-    }
-    cp_async_commit();  // empty groups keep the group arithmetic uniform
-  };
-  auto issue_gather = [&](int k) {
-    if (k >= 0 && k < ntile) {
-      uint8_t* st = ring + (k % kStages) * STAGE;
-      const int32_t col = reinterpret_cast<const int32_t*>(st)[lane];
-      uint8_t* dst = st + REC;
-#pragma unroll
-      for (int i = 0; i < CH; ++i) {
-        const int ci = lane + 32 * i;
-        const int row = ci / CH, ch = ci % CH;
-        const int src = __shfl_sync(0xFFFFFFFFu, col, row);
-        cp_async16(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16, pb + static_cast<size_t>(src) * BYTES + ch * 16);
-      }
-    }
-    cp_async_commit();
-  };
-
-  // Uniform iterations k = -kRecAhead .. ntile-1, two commit groups each (empty when out of
-  // range).  Newest-first the pending groups before "wait<4>" are
-  //   [rec(k+4), gat(k+1), rec(k+3), gat(k), rec(k+2), ...]   -> rec(k+2) has landed
-  // and after issuing gat(k+2)
-  //   [gat(k+2), rec(k+4), gat(k+1), rec(k+3), gat(k), ...]   -> gat(k) has landed.
-  static_assert(kRecAhead == 4 && kGatherAhead == 2 && kStages == kRecAhead + 1, "group arithmetic");
-  for (int k = -kRecAhead; k < ntile; ++k) {
-    issue_record(k + kRecAhead);
-    cp_async_wait<4>();
-    __syncwarp();
-    issue_gather(k + kGatherAhead);
-    cp_async_wait<4>();
-    __syncwarp();
-    if (k < 0) continue;
-    uint8_t* st = ring + (k % kStages) * STAGE;
-    uint32_t a[NCOMP][4], meta[NCOMP];
-#pragma unroll
-    for (int c = 0; c < NCOMP; ++c) {
-      // A rows of 32 B; the 16-B halves of row r are stored swapped when (r >> 2) & 1
-      const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
-      const int half = lane >> 4;
-      ldmatrix_x4(a[c], st + 128 + 576 * c + r * 32 + ((half ^ ((r >> 2) & 1)) * 16));
-      meta[c] = reinterpret_cast<const uint32_t*>(st + 640 + 576 * c)[g * 2 + (t & 1)];
-    }
-    const uint8_t* B = st + REC;
-#pragma unroll
-    for (int nb = 0; nb < NB; ++nb) {
-      uint32_t b[4];
-      ldmatrix_x4_trans(b, B + lane * BYTES + chunk_swizzle<CH>(nb, lane) * 16);
-      const int ai = SPLIT ? (nb % NA) : nb;
-#pragma unroll
-      for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
-    }
-    __syncwarp();  // stage k is reused by record(k + kStages) next iteration
-  }
-  cp_async_wait<0>();
-
-  if (item.split >= 0) {
-    // split group: publish this chunk, the last chunk to arrive reduces all in order
-    const SplitGroup sg = v.splits[item.split];
+  if (split >= 0) {
+    const SplitGroup sg = v.splits[split];
     const int chunk = static_cast<int>((t0 - v.group_offsets[gidx]) / kChunkTiles);
     float* mine = v.partials + static_cast<size_t>(sg.first_slot + chunk) * kPartialFloats * 32;
 #pragma unroll
@@ -165,7 +78,7 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
     __threadfence();
     __syncwarp();
     int prior = 0;
-    if (lane == 0) prior = atomicAdd(&v.counters[item.split], 1);
+    if (lane == 0) prior = atomicAdd(&v.counters[split], 1);
     prior = __shfl_sync(0xFFFFFFFFu, prior, 0);
     if (prior != sg.nchunks - 1) return;
     __threadfence();
@@ -184,9 +97,8 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 #pragma unroll
           for (int i = 0; i < 4; ++i) acc[c][a2][i] += __ldcg(src + ((c * NA + a2) * 4 + i) * 32 + lane);
     }
-    if (lane == 0) v.counters[item.split] = 0;  // ready for the next launch
+    if (lane == 0) v.counters[split] = 0;  // ready for the next launch
   }
-
   const int32_t rows[2] = {v.group_rows[gidx * 16 + g], v.group_rows[gidx * 16 + g + 8]};
   float scale = o.scale_mul;
   if (o.scale_ptr) {
@@ -247,8 +159,134 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 }
 
 template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
+__global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpView v, const __half* __restrict__ panel,
+                                                                         InterpOut o) {
+  constexpr int BYTES = ROWH * 2;
+  constexpr int CH = BYTES / 16;
+  constexpr int NB = ROWH / 8;
+  constexpr int NA = SPLIT ? NB / 2 : NB;
+  constexpr int NACC = NCOMP * NA * 4;
+  constexpr int REC = 128 + 576 * NCOMP;          // record bytes staged (components used here)
+  constexpr int STAGE = REC + 32 * BYTES;
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  static_assert(NACC <= kPartialFloats, "partials slot too small");
+  static_assert(REC % 16 == 0 && STAGE % 16 == 0, "16-byte stages");
+  static_assert(kRecAhead == 4 && kGatherAhead == 2 && kStages == kRecAhead + 1, "group arithmetic");
+  extern __shared__ __align__(128) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wid = blockIdx.x * kInterpWarps + warp;
+  if (wid >= v.n_warps) return;
+  const int2 range = v.warp_ranges[wid];
+  uint8_t* ring = smem + warp * kStages * STAGE;
+  const uint8_t* pb = reinterpret_cast<const uint8_t*>(panel);
+  const int g = lane >> 2, t = lane & 3;
+
+  float acc[NCOMP][NA][4];
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c)
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[c][a][i] = 0.f;
+
+  for (int base = range.x; base < range.y; base += 32) {
+    // up to 32 items of this warp's run, one descriptor per lane
+    const int nitems = min(32, range.y - base);
+    WorkItem it{0, 0u, 0u, -1};
+    if (lane < nitems) it = v.items[base + lane];
+    const int cnt = lane < nitems ? static_cast<int>(it.t1 - it.t0) : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, off);
+      if (lane >= off) incl += y;
+    }
+    const int start = incl - cnt;
+    const int total = __shfl_sync(FULL, incl, 31);
+    // stream position -> (lane slot of its item, tile index); p must be in [0, total)
+    auto slot_of = [&](int p) {
+      const unsigned m = __ballot_sync(FULL, cnt > 0 && start <= p);
+      return 31 - __clz(m);
+    };
+    auto issue_record = [&](int p) {
+      if (p >= 0 && p < total) {
+        const int sl = slot_of(p);
+        const uint32_t tile = __shfl_sync(FULL, it.t0, sl) + static_cast<uint32_t>(p - __shfl_sync(FULL, start, sl));
+        const uint8_t* src = v.records + static_cast<size_t>(tile) * v.rec_bytes;
+        uint8_t* dst = ring + (p % kStages) * STAGE;
+        for (int c = lane; c < REC / 16; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
+      }
+      cp_async_commit();  // empty groups keep the group arithmetic uniform
+    };
+    auto issue_gather = [&](int p) {
+      if (p >= 0 && p < total) {
+        uint8_t* st = ring + (p % kStages) * STAGE;
+        const int32_t col = reinterpret_cast<const int32_t*>(st)[lane];
+        uint8_t* dst = st + REC;
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          const int ci = lane + 32 * i;
+          const int row = ci / CH, ch = ci % CH;
+          const int src = __shfl_sync(FULL, col, row);
+          cp_async16(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16,
+                     pb + static_cast<size_t>(src) * BYTES + ch * 16);
+        }
+      }
+      cp_async_commit();
+    };
+    // Uniform iterations p = -kRecAhead .. total-1, two commit groups each (empty when out of
+    // range).  Newest-first the pending groups before the first "wait<4>" are
+    //   [rec(p+4), gat(p+1), rec(p+3), gat(p), rec(p+2), ...]   -> rec(p+2) has landed
+    // and after issuing gat(p+2)
+    //   [gat(p+2), rec(p+4), gat(p+1), rec(p+3), gat(p), ...]   -> gat(p) has landed.
+    for (int p = -kRecAhead; p < total; ++p) {
+      issue_record(p + kRecAhead);
+      cp_async_wait<4>();
+      __syncwarp();
+      issue_gather(p + kGatherAhead);
+      cp_async_wait<4>();
+      __syncwarp();
+      if (p < 0) continue;
+      uint8_t* st = ring + (p % kStages) * STAGE;
+      uint32_t a[NCOMP][4], meta[NCOMP];
+#pragma unroll
+      for (int c = 0; c < NCOMP; ++c) {
+        // A rows of 32 B; the 16-B halves of row r are stored swapped when (r >> 2) & 1
+        const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
+        const int half = lane >> 4;
+        ldmatrix_x4(a[c], st + 128 + 576 * c + r * 32 + ((half ^ ((r >> 2) & 1)) * 16));
+        meta[c] = reinterpret_cast<const uint32_t*>(st + 640 + 576 * c)[g * 2 + (t & 1)];
+      }
+      const uint8_t* B = st + REC;
+#pragma unroll
+      for (int nb = 0; nb < NB; ++nb) {
+        uint32_t b[4];
+        ldmatrix_x4_trans(b, B + lane * BYTES + chunk_swizzle<CH>(nb, lane) * 16);
+        const int ai = SPLIT ? (nb % NA) : nb;
+#pragma unroll
+        for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
+      }
+      __syncwarp();  // stage p is reused by record(p + kStages) next iteration
+      const int sl = slot_of(p);
+      if (p == __shfl_sync(FULL, incl, sl) - 1) {  // last tile of its item
+        interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ>(acc, v, o, __shfl_sync(FULL, it.group, sl),
+                                                       __shfl_sync(FULL, it.split, sl),
+                                                       __shfl_sync(FULL, it.t0, sl), lane);
+#pragma unroll
+        for (int c = 0; c < NCOMP; ++c)
+#pragma unroll
+          for (int a2 = 0; a2 < NA; ++a2)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[c][a2][i] = 0.f;
+      }
+    }
+    cp_async_wait<0>();
+  }
+}
+
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
 static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
-  const int blocks = (v.n_items + kInterpWarps - 1) / kInterpWarps;
+  const int blocks = (v.n_warps + kInterpWarps - 1) / kInterpWarps;
   const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (128 + 576 * NCOMP + 32 * ROWH * 2);
   auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -266,6 +304,31 @@ static void dispatch_epi(const InterpView& v, const __half* panel, int epi, bool
     if (epi == EPI_SAMPLES) launch_interp_t<ROWH, true, 1, EPI_SAMPLES, false>(v, panel, o, s);
     else if (epi == EPI_PANEL) launch_interp_t<ROWH, true, 1, EPI_PANEL, false>(v, panel, o, s);
     else launch_interp_t<ROWH, true, 1, EPI_GRID, false>(v, panel, o, s);
+  }
+}
+
+static int sm_count();
+
+template <int ROWH, int NCOMP>
+static int resident_warps_t() {
+  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (128 + 576 * NCOMP + 32 * ROWH * 2);
+  auto k = interp_mmasp_kernel<ROWH, true, NCOMP, EPI_GRID, NCOMP == 2>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kInterpWarps * 32, smem);
+  return std::max(1, per_sm) * kInterpWarps * sm_count();
+}
+
+int interp_resident_warps(int rowh, int ncomp) {
+  switch (rowh * 4 + ncomp) {
+    case 16 * 4 + 1: return resident_warps_t<16, 1>();
+    case 16 * 4 + 2: return resident_warps_t<16, 2>();
+    case 32 * 4 + 1: return resident_warps_t<32, 1>();
+    case 32 * 4 + 2: return resident_warps_t<32, 2>();
+    case 48 * 4 + 1: return resident_warps_t<48, 1>();
+    case 48 * 4 + 2: return resident_warps_t<48, 2>();
+    case 64 * 4 + 1: return resident_warps_t<64, 1>();
+    default: return resident_warps_t<64, 2>();
   }
 }
 
@@ -329,6 +392,24 @@ __device__ __forceinline__ void cp_async_bytes(void* dst, const void* src, int b
   for (int i = threadIdx.x * 16; i < bytes; i += blockDim.x * 16) cp_async16(d + i, q + i);
 }
 
+// [rows][C] complex slabs in shared memory hold each row's C/2 16-byte chunks XOR-swizzled
+// by the row index, so a warp reading one coil down 32 consecutive rows touches distinct
+// banks (unswizzled, 64-byte rows make that a 16-way conflict).
+__device__ __forceinline__ int slab_swz(int n, int chn) {
+  return chn == 2 ? (n >> 2) & 1 : chn == 4 ? (n >> 1) & 3 : chn == 8 ? (n & 7) : 0;
+}
+__device__ __forceinline__ int slab_idx(int n, int c, int C) {
+  return n * C + 2 * ((c >> 1) ^ slab_swz(n, C >> 1)) + (c & 1);
+}
+// copy `rows` contiguous rows of C complex values into a swizzled slab (all threads)
+__device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, int rows, int C) {
+  const int chn = C >> 1;
+  for (int q = threadIdx.x; q < rows * chn; q += blockDim.x) {
+    const int n = q / chn, k = q - n * chn;
+    cp_async16(dst + n * C + 2 * (k ^ slab_swz(n, chn)), src + n * C + 2 * k);
+  }
+}
+
 // The four FFT stages are persistent CTAs (one warp per coil) walking their items with a
 // double-buffered cp.async input slab: item i+1 streams in while item i is transformed.
 
@@ -351,8 +432,8 @@ __global__ void __launch_bounds__(512) fwd_rows_kernel(FftArgs f, const float2* 
   const int in_bytes = in_f2 * 8 + N * 4;
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* inb = reinterpret_cast<uint8_t*>(tw_s + G);   // [2][in_bytes]
-  float2* out_s = reinterpret_cast<float2*>(inb + 2 * in_bytes);  // [G][C]
-  float2* scr = out_s + G * C;                           // [C][SCR]
+  float2* out_s = reinterpret_cast<float2*>(inb + 2 * in_bytes);  // [G][C+1] (padded)
+  float2* scr = out_s + G * (C + 1);                     // [C][SCR]
   __shared__ double red[33];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
@@ -435,12 +516,12 @@ __global__ void __launch_bounds__(512) fwd_rows_kernel(FftArgs f, const float2* 
       }
       warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
 #pragma unroll
-      for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * C + c] = v[m];
+      for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * (C + 1) + c] = v[m];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < G * C; e += blockDim.x) {
       const int q1 = e / C, c = e - q1 * C;
-      z1[(static_cast<size_t>(q1) * N + i0) * C + c] = out_s[e];
+      z1[(static_cast<size_t>(q1) * N + i0) * C + c] = out_s[q1 * (C + 1) + c];
     }
   }
 }
@@ -456,11 +537,12 @@ __global__ void __launch_bounds__(512) fwd_cols_kernel(FftArgs f, const float2* 
   float2* tw_s = reinterpret_cast<float2*>(sm);
   float2* inb = tw_s + G;                              // [2][N*C]
   float2* scr = inb + 2 * N * C;                       // [C][SCR]
-  uint32_t* out_s = reinterpret_cast<uint32_t*>(scr + C * FftSmem<G>::SCR);  // [G][2C] half2
+  uint32_t* out_s = reinterpret_cast<uint32_t*>(scr + C * FftSmem<G>::SCR);  // [G][2C+1] half2 (padded)
+  const int OP = 2 * C + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
   auto prefetch = [&](int q1, int buf) {
-    cp_async_bytes(inb + buf * N * C, z1 + static_cast<size_t>(q1) * N * C, N * C * 8);
+    cp_async_slab(inb + buf * N * C, z1 + static_cast<size_t>(q1) * N * C, N, C);
     cp_async_commit();
   };
   int buf = 0;
@@ -483,7 +565,7 @@ __global__ void __launch_bounds__(512) fwd_cols_kernel(FftArgs f, const float2* 
         const int n = lane + 32 * j;
         int i0 = n + f.shift;
         if (i0 >= G) i0 -= G;
-        v[j] = i0 < N ? in_s[i0 * C + c] : make_float2(0.f, 0.f);
+        v[j] = i0 < N ? in_s[slab_idx(i0, c, C)] : make_float2(0.f, 0.f);
       }
       warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
 #pragma unroll
@@ -492,14 +574,16 @@ __global__ void __launch_bounds__(512) fwd_cols_kernel(FftArgs f, const float2* 
         __half hr, rr, hi, ri;
         split_hi_res(v[m].x, hr, rr);
         split_hi_res(v[m].y, hi, ri);
-        out_s[q0 * 2 * C + c] = pack_half2(hr, hi);
-        out_s[q0 * 2 * C + C + c] = pack_half2(rr, ri);
+        out_s[q0 * OP + c] = pack_half2(hr, hi);
+        out_s[q0 * OP + C + c] = pack_half2(rr, ri);
       }
     }
     __syncthreads();
-    const int4* src = reinterpret_cast<const int4*>(out_s);
-    int4* dst = reinterpret_cast<int4*>(panel + static_cast<size_t>(q1) * G * 4 * C);
-    for (int i = threadIdx.x; i < G * C / 2; i += blockDim.x) dst[i] = src[i];
+    uint32_t* dst = reinterpret_cast<uint32_t*>(panel + static_cast<size_t>(q1) * G * 4 * C);
+    for (int i = threadIdx.x; i < G * 2 * C; i += blockDim.x) {
+      const int q0 = i / (2 * C), w = i - q0 * 2 * C;
+      dst[i] = out_s[q0 * OP + w];
+    }
   }
 }
 
@@ -548,13 +632,13 @@ __global__ void __launch_bounds__(512) inv_cols_kernel(FftArgs f, const float2* 
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* inb = tw_s + G;                // [2][G*C]
-  float2* out_s = inb + 2 * G * C;       // [N][C]
-  float2* scr = out_s + N * C;           // [C][SCR]
+  float2* inb = tw_s + G;                // [2][G*C] swizzled slabs
+  float2* out_s = inb + 2 * G * C;       // [N][C+1] (padded)
+  float2* scr = out_s + N * (C + 1);     // [C][SCR]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(tw_s, f.tw, G);
   auto prefetch = [&](int q1, int buf) {
-    cp_async_bytes(inb + buf * G * C, grid + static_cast<size_t>(q1) * G * C, G * C * 8);
+    cp_async_slab(inb + buf * G * C, grid + static_cast<size_t>(q1) * G * C, G, C);
     cp_async_commit();
   };
   int buf = 0;
@@ -573,19 +657,21 @@ __global__ void __launch_bounds__(512) inv_cols_kernel(FftArgs f, const float2* 
       const int c = warp;
       float2 v[P];
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = in_s[(lane + 32 * j) * C + c];
+      for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
       warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
 #pragma unroll
       for (int m = 0; m < P; ++m) {
         int i0 = warp_fft_out_index<G>(m) + f.shift;
         if (i0 >= G) i0 -= G;
-        if (i0 < N) out_s[i0 * C + c] = v[m];
+        if (i0 < N) out_s[i0 * (C + 1) + c] = v[m];
       }
     }
     __syncthreads();
-    const float4* src = reinterpret_cast<const float4*>(out_s);
-    float4* dst = reinterpret_cast<float4*>(w1 + static_cast<size_t>(q1) * N * C);
-    for (int i = threadIdx.x; i < N * C / 2; i += blockDim.x) dst[i] = src[i];
+    float2* dst = w1 + static_cast<size_t>(q1) * N * C;
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
+      const int i0 = i / C, c = i - i0 * C;
+      dst[i] = out_s[i0 * (C + 1) + c];
+    }
   }
 }
 
@@ -613,11 +699,11 @@ __global__ void __launch_bounds__(512) inv_rows_kernel(FftArgs f, const float2* 
   else factor = inv_scale2 / st->sigma_y;
   auto prefetch = [&](int i0, int buf) {
     float2* dst = inb + buf * G * C;
-    // G runs of C complex values (8C bytes each, 16-byte aligned for even C)
-    const int chunks_per_run = C / 2;
-    for (int e = threadIdx.x; e < G * chunks_per_run; e += blockDim.x) {
-      const int q1 = e / chunks_per_run, k = e - q1 * chunks_per_run;
-      cp_async16(dst + q1 * C + 2 * k, w1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * k);
+    // G runs of C complex values (8C bytes each, 16-byte aligned for even C), swizzled
+    const int chn = C / 2;
+    for (int e = threadIdx.x; e < G * chn; e += blockDim.x) {
+      const int q1 = e / chn, k = e - q1 * chn;
+      cp_async16(dst + q1 * C + 2 * (k ^ slab_swz(q1, chn)), w1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * k);
     }
     cp_async_commit();
   };
@@ -637,7 +723,7 @@ __global__ void __launch_bounds__(512) inv_rows_kernel(FftArgs f, const float2* 
       const int c = warp;
       float2 v[P];
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = in_s[(lane + 32 * j) * C + c];
+      for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
       warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
 #pragma unroll
       for (int m = 0; m < P; ++m) {
@@ -729,16 +815,17 @@ __global__ void cg_finish_kernel(int N, const double* __restrict__ rr_parts, CgS
 template <int G>
 static size_t fwd_rows_smem(const FftArgs& f) {
   const size_t in_bytes = static_cast<size_t>(2 + f.C) * f.N * 8 + static_cast<size_t>(f.N) * 4;
-  return sizeof(float2) * G + 2 * in_bytes + sizeof(float2) * (static_cast<size_t>(G) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR);
+  return sizeof(float2) * G + 2 * in_bytes +
+         sizeof(float2) * (static_cast<size_t>(G) * (f.C + 1) + static_cast<size_t>(f.C) * FftSmem<G>::SCR);
 }
 template <int G>
 static size_t fwd_cols_smem(const FftArgs& f) {
   return sizeof(float2) * (G + 2 * static_cast<size_t>(f.N) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR) +
-         sizeof(uint32_t) * static_cast<size_t>(G) * 2 * f.C;
+         sizeof(uint32_t) * static_cast<size_t>(G) * (2 * f.C + 1);
 }
 template <int G>
 static size_t inv_cols_smem(const FftArgs& f) {
-  return sizeof(float2) * (G + 2 * static_cast<size_t>(G) * f.C + static_cast<size_t>(f.N) * f.C +
+  return sizeof(float2) * (G + 2 * static_cast<size_t>(G) * f.C + static_cast<size_t>(f.N) * (f.C + 1) +
                            static_cast<size_t>(f.C) * FftSmem<G>::SCR);
 }
 template <int G>

@@ -52,6 +52,8 @@ struct InterpView {
   const SplitGroup* splits = nullptr;
   int32_t* counters = nullptr;          // one per split group, zero between launches
   float* partials = nullptr;            // [slots][kPartialFloats][32]
+  const int2* warp_ranges = nullptr;    // per persistent warp: [first item, end item)
+  int32_t n_warps = 0;
   int32_t groups = 0;
   int32_t n_items = 0;
   int32_t ncomp = 0;
@@ -84,6 +86,10 @@ void set_twiddle_constants(cudaStream_t s);
 
 void launch_interp(const InterpView& v, const __half* panel, int rowh, bool split, int epi, bool conj,
                    const InterpOut& o, cudaStream_t s);
+// warps the persistent interpolation kernel keeps resident on this device for a panel row
+// width / component count (used to cut the item list into per-warp runs)
+int interp_resident_warps(int rowh, int ncomp);
+constexpr int kInterpWarpsPerCta = 4;
 
 void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t s);
 

@@ -69,7 +69,7 @@ struct HostView {
 };
 
 struct DevView {
-  DeviceBuffer records, offsets, rows, items, splits, counters, partials;
+  DeviceBuffer records, offsets, rows, items, splits, counters, partials, ranges;
   InterpView v;
   int64_t tiles = 0, groups = 0, active_rows = 0, nnz = 0, output_size = 0, n_cols = 0;
   bool present = false;
@@ -158,6 +158,23 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
                              std::min<uint32_t>(b, a + (k + 1) * kChunkTiles), sid});
   }
   big.insert(big.end(), small.begin(), small.end());
+  // persistent warps: contiguous runs of items with about the same number of tiles each
+  const int resident = interp_resident_warps(4 * P->C, ncomp);
+  int64_t total_tiles = 0;
+  for (const WorkItem& w : big) total_tiles += w.t1 - w.t0;
+  const int64_t target = std::max<int64_t>(1, (total_tiles + resident - 1) / resident);
+  std::vector<int2> ranges;
+  int64_t acc_tiles = 0;
+  int first = 0;
+  for (int i = 0; i < static_cast<int>(big.size()); ++i) {
+    acc_tiles += big[i].t1 - big[i].t0;
+    if (acc_tiles >= target) {
+      ranges.push_back(make_int2(first, i + 1));
+      first = i + 1;
+      acc_tiles = 0;
+    }
+  }
+  if (first < static_cast<int>(big.size())) ranges.push_back(make_int2(first, static_cast<int>(big.size())));
   d.records.upload(records);
   d.offsets.upload(h.group_offsets);
   d.rows.upload(rows);
@@ -170,6 +187,9 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   d.v.counters = d.counters.as<int32_t>();
   d.v.partials = d.partials.as<float>();
   d.v.n_items = static_cast<int32_t>(big.size());
+  d.ranges.upload(ranges);
+  d.v.warp_ranges = d.ranges.as<int2>();
+  d.v.n_warps = static_cast<int32_t>(ranges.size());
   d.v.records = d.records.as<uint8_t>();
   d.v.group_offsets = d.offsets.as<uint32_t>();
   d.v.group_rows = d.rows.as<int32_t>();
