@@ -63,8 +63,9 @@ constexpr int kGatherAhead = 2;
 // epilogue.
 template <int ROWH, int NCOMP, int NA, int EPI, bool CONJ>
 __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], const InterpView& v,
-                                                   const InterpOut& o, int gidx, int split, uint32_t t0, int lane) {
-  const int g = lane >> 2, t = lane & 3;
+                                                   const InterpOut& o, int gidx, int split, uint32_t t0, int lane,
+                                                   const int32_t (&rows)[2], const float (&wrow)[2], float scale) {
+  const int t = lane & 3;
   if (split >= 0) {
     const SplitGroup sg = v.splits[split];
     const int chunk = static_cast<int>((t0 - v.group_offsets[gidx]) / kChunkTiles);
@@ -99,12 +100,6 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
     }
     if (lane == 0) v.counters[split] = 0;  // ready for the next launch
   }
-  const int32_t rows[2] = {v.group_rows[gidx * 16 + g], v.group_rows[gidx * 16 + g + 8]};
-  float scale = o.scale_mul;
-  if (o.scale_ptr) {
-    const float sp = *o.scale_ptr;
-    scale *= o.scale_inv ? 1.0f / sp : sp;
-  }
   if constexpr (EPI == EPI_RAW) {
 #pragma unroll
     for (int hr = 0; hr < 2; ++hr) {
@@ -121,10 +116,7 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
     for (int hr = 0; hr < 2; ++hr) {
       const int32_t row = rows[hr];
       if (row < 0) continue;
-      float w = scale;
-      if constexpr (EPI == EPI_PANEL) {
-        if (o.density) w *= o.density[row];
-      }
+      const float w = scale * wrow[hr];
 #pragma unroll
       for (int a2 = 0; a2 < NA; ++a2) {
         const int coil = 4 * a2 + t;
@@ -180,6 +172,14 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   uint8_t* ring = smem + warp * kStages * STAGE;
   const uint8_t* pb = reinterpret_cast<const uint8_t*>(panel);
   const int g = lane >> 2, t = lane & 3;
+  float scale = o.scale_mul;
+  if (o.scale_ptr) {
+    const float sp = *o.scale_ptr;
+    scale *= o.scale_inv ? 1.0f / sp : sp;
+  }
+  // epilogue inputs of the open item, loaded at its first tile and consumed at its last
+  int32_t rows[2] = {-1, -1};
+  float wrow[2] = {1.f, 1.f};
 
   float acc[NCOMP][NA][4];
 #pragma unroll
@@ -247,6 +247,19 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
       cp_async_wait<4>();
       __syncwarp();
       if (p < 0) continue;
+      const int sl = slot_of(p);
+      const int first = __shfl_sync(FULL, start, sl), last = __shfl_sync(FULL, incl, sl) - 1;
+      if (p == first) {  // first tile of its item: prefetch the epilogue's row ids
+        const int gi = __shfl_sync(FULL, it.group, sl);
+        rows[0] = __ldg(v.group_rows + gi * 16 + g);
+        rows[1] = __ldg(v.group_rows + gi * 16 + g + 8);
+      }
+      if constexpr (EPI == EPI_PANEL) {  // density weights one tile later (they need the row ids)
+        if (o.density && p == min(first + 1, last)) {
+          wrow[0] = rows[0] >= 0 ? __ldg(o.density + rows[0]) : 1.f;
+          wrow[1] = rows[1] >= 0 ? __ldg(o.density + rows[1]) : 1.f;
+        }
+      }
       uint8_t* st = ring + (p % kStages) * STAGE;
       uint32_t a[NCOMP][4], meta[NCOMP];
 #pragma unroll
@@ -267,11 +280,10 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
         for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
       }
       __syncwarp();  // stage p is reused by record(p + kStages) next iteration
-      const int sl = slot_of(p);
-      if (p == __shfl_sync(FULL, incl, sl) - 1) {  // last tile of its item
+      if (p == last) {  // last tile of its item
         interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ>(acc, v, o, __shfl_sync(FULL, it.group, sl),
                                                        __shfl_sync(FULL, it.split, sl),
-                                                       __shfl_sync(FULL, it.t0, sl), lane);
+                                                       __shfl_sync(FULL, it.t0, sl), lane, rows, wrow, scale);
 #pragma unroll
         for (int c = 0; c < NCOMP; ++c)
 #pragma unroll
