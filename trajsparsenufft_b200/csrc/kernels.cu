@@ -63,13 +63,13 @@ constexpr int kGatherAhead = 2;
 // epilogue.
 template <int ROWH, int NCOMP, int NA, int EPI, bool CONJ>
 __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], const InterpView& v,
-                                                   const InterpOut& o, int gidx, int split, uint32_t t0, int lane,
+                                                   const InterpOut& o, const RecordInfo& info, int lane,
                                                    const int32_t (&rows)[2], const float (&wrow)[2], float scale) {
   const int t = lane & 3;
-  if (split >= 0) {
-    const SplitGroup sg = v.splits[split];
-    const int chunk = static_cast<int>((t0 - v.group_offsets[gidx]) / kChunkTiles);
-    float* mine = v.partials + static_cast<size_t>(sg.first_slot + chunk) * kPartialFloats * 32;
+  if (info.split >= 0) {
+    const int split = info.split;
+    const int chunk = info.chunk & 0xFFFF, nchunks = info.chunk >> 16;
+    float* mine = v.partials + static_cast<size_t>(info.first_slot + chunk) * kPartialFloats * 32;
 #pragma unroll
     for (int c = 0; c < NCOMP; ++c)
 #pragma unroll
@@ -81,7 +81,7 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
     int prior = 0;
     if (lane == 0) prior = atomicAdd(&v.counters[split], 1);
     prior = __shfl_sync(0xFFFFFFFFu, prior, 0);
-    if (prior != sg.nchunks - 1) return;
+    if (prior != nchunks - 1) return;
     __threadfence();
 #pragma unroll
     for (int c = 0; c < NCOMP; ++c)
@@ -89,8 +89,8 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
       for (int a2 = 0; a2 < NA; ++a2)
 #pragma unroll
         for (int i = 0; i < 4; ++i) acc[c][a2][i] = 0.f;
-    for (int k = 0; k < sg.nchunks; ++k) {
-      const float* src = v.partials + static_cast<size_t>(sg.first_slot + k) * kPartialFloats * 32;
+    for (int k = 0; k < nchunks; ++k) {
+      const float* src = v.partials + static_cast<size_t>(info.first_slot + k) * kPartialFloats * 32;
 #pragma unroll
       for (int c = 0; c < NCOMP; ++c)
 #pragma unroll
@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   constexpr int NB = ROWH / 8;
   constexpr int NA = SPLIT ? NB / 2 : NB;
   constexpr int NACC = NCOMP * NA * 4;
-  constexpr int REC = 128 + 576 * NCOMP;          // record bytes staged (components used here)
+  constexpr int INFO = 128 + 576 * NCOMP;         // RecordInfo offset in the record
+  constexpr int REC = record_bytes(NCOMP);        // record bytes (all staged)
   constexpr int STAGE = REC + 32 * BYTES;
   constexpr unsigned FULL = 0xFFFFFFFFu;
   static_assert(NACC <= kPartialFloats, "partials slot too small");
@@ -169,17 +170,17 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   const int wid = blockIdx.x * kInterpWarps + warp;
   if (wid >= v.n_warps) return;
   const int2 range = v.warp_ranges[wid];
+  const int n = range.y - range.x;
+  const uint8_t* recs = v.records + static_cast<size_t>(range.x) * REC;
   uint8_t* ring = smem + warp * kStages * STAGE;
   const uint8_t* pb = reinterpret_cast<const uint8_t*>(panel);
-  const int g = lane >> 2, t = lane & 3;
+  const int g = lane >> 2;
   float scale = o.scale_mul;
   if (o.scale_ptr) {
     const float sp = *o.scale_ptr;
     scale *= o.scale_inv ? 1.0f / sp : sp;
   }
-  // epilogue inputs of the open item, loaded at its first tile and consumed at its last
-  int32_t rows[2] = {-1, -1};
-  float wrow[2] = {1.f, 1.f};
+  float wrow[2] = {1.f, 1.f};  // density of the open item's rows (EPI_PANEL)
 
   float acc[NCOMP][NA][4];
 #pragma unroll
@@ -189,117 +190,95 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[c][a][i] = 0.f;
 
-  for (int base = range.x; base < range.y; base += 32) {
-    // up to 32 items of this warp's run, one descriptor per lane
-    const int nitems = min(32, range.y - base);
-    WorkItem it{0, 0u, 0u, -1};
-    if (lane < nitems) it = v.items[base + lane];
-    const int cnt = lane < nitems ? static_cast<int>(it.t1 - it.t0) : 0;
-    int incl = cnt;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const int y = __shfl_up_sync(FULL, incl, off);
-      if (lane >= off) incl += y;
+  // k-th record of this warp -> its ring stage
+  auto issue_record = [&](int k) {
+    if (k < n) {
+      const uint8_t* src = recs + static_cast<size_t>(k) * REC;
+      uint8_t* dst = ring + (k % kStages) * STAGE;
+      for (int c = lane; c < REC / 16; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
     }
-    const int start = incl - cnt;
-    const int total = __shfl_sync(FULL, incl, 31);
-    // stream position -> (lane slot of its item, tile index); p must be in [0, total)
-    auto slot_of = [&](int p) {
-      const unsigned m = __ballot_sync(FULL, cnt > 0 && start <= p);
-      return 31 - __clz(m);
-    };
-    auto issue_record = [&](int p) {
-      if (p >= 0 && p < total) {
-        const int sl = slot_of(p);
-        const uint32_t tile = __shfl_sync(FULL, it.t0, sl) + static_cast<uint32_t>(p - __shfl_sync(FULL, start, sl));
-        const uint8_t* src = v.records + static_cast<size_t>(tile) * v.rec_bytes;
-        uint8_t* dst = ring + (p % kStages) * STAGE;
-        for (int c = lane; c < REC / 16; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
-      }
-      cp_async_commit();  // empty groups keep the group arithmetic uniform
-    };
-    auto issue_gather = [&](int p) {
-      if (p >= 0 && p < total) {
-        uint8_t* st = ring + (p % kStages) * STAGE;
-        const int32_t col = reinterpret_cast<const int32_t*>(st)[lane];
-        uint8_t* dst = st + REC;
+    cp_async_commit();  // empty groups keep the group arithmetic uniform
+  };
+  auto issue_gather = [&](int k) {
+    if (k >= 0 && k < n) {
+      uint8_t* st = ring + (k % kStages) * STAGE;
+      const int32_t col = reinterpret_cast<const int32_t*>(st)[lane];
+      uint8_t* dst = st + REC;
 #pragma unroll
-        for (int i = 0; i < CH; ++i) {
-          const int ci = lane + 32 * i;
-          const int row = ci / CH, ch = ci % CH;
-          const int src = __shfl_sync(FULL, col, row);
-          cp_async16(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16,
-                     pb + static_cast<size_t>(src) * BYTES + ch * 16);
-        }
-      }
-      cp_async_commit();
-    };
-    // Uniform iterations p = -kRecAhead .. total-1, two commit groups each (empty when out of
-    // range).  Newest-first the pending groups before the first "wait<4>" are
-    //   [rec(p+4), gat(p+1), rec(p+3), gat(p), rec(p+2), ...]   -> rec(p+2) has landed
-    // and after issuing gat(p+2)
-    //   [gat(p+2), rec(p+4), gat(p+1), rec(p+3), gat(p), ...]   -> gat(p) has landed.
-    for (int p = -kRecAhead; p < total; ++p) {
-      issue_record(p + kRecAhead);
-      cp_async_wait<4>();
-      __syncwarp();
-      issue_gather(p + kGatherAhead);
-      cp_async_wait<4>();
-      __syncwarp();
-      if (p < 0) continue;
-      const int sl = slot_of(p);
-      const int first = __shfl_sync(FULL, start, sl), last = __shfl_sync(FULL, incl, sl) - 1;
-      if (p == first) {  // first tile of its item: prefetch the epilogue's row ids
-        const int gi = __shfl_sync(FULL, it.group, sl);
-        rows[0] = __ldg(v.group_rows + gi * 16 + g);
-        rows[1] = __ldg(v.group_rows + gi * 16 + g + 8);
-      }
-      if constexpr (EPI == EPI_PANEL) {  // density weights one tile later (they need the row ids)
-        if (o.density && p == min(first + 1, last)) {
-          wrow[0] = rows[0] >= 0 ? __ldg(o.density + rows[0]) : 1.f;
-          wrow[1] = rows[1] >= 0 ? __ldg(o.density + rows[1]) : 1.f;
-        }
-      }
-      uint8_t* st = ring + (p % kStages) * STAGE;
-      uint32_t a[NCOMP][4], meta[NCOMP];
-#pragma unroll
-      for (int c = 0; c < NCOMP; ++c) {
-        // A rows of 32 B; the 16-B halves of row r are stored swapped when (r >> 2) & 1
-        const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
-        const int half = lane >> 4;
-        ldmatrix_x4(a[c], st + 128 + 576 * c + r * 32 + ((half ^ ((r >> 2) & 1)) * 16));
-        meta[c] = reinterpret_cast<const uint32_t*>(st + 640 + 576 * c)[g * 2 + (t & 1)];
-      }
-      const uint8_t* B = st + REC;
-#pragma unroll
-      for (int nb = 0; nb < NB; ++nb) {
-        uint32_t b[4];
-        ldmatrix_x4_trans(b, B + lane * BYTES + chunk_swizzle<CH>(nb, lane) * 16);
-        const int ai = SPLIT ? (nb % NA) : nb;
-#pragma unroll
-        for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
-      }
-      __syncwarp();  // stage p is reused by record(p + kStages) next iteration
-      if (p == last) {  // last tile of its item
-        interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ>(acc, v, o, __shfl_sync(FULL, it.group, sl),
-                                                       __shfl_sync(FULL, it.split, sl),
-                                                       __shfl_sync(FULL, it.t0, sl), lane, rows, wrow, scale);
-#pragma unroll
-        for (int c = 0; c < NCOMP; ++c)
-#pragma unroll
-          for (int a2 = 0; a2 < NA; ++a2)
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[c][a2][i] = 0.f;
+      for (int i = 0; i < CH; ++i) {
+        const int ci = lane + 32 * i;
+        const int row = ci / CH, ch = ci % CH;
+        const int src = __shfl_sync(FULL, col, row);
+        cp_async16_zfill(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16,
+                         pb + static_cast<size_t>(max(src, 0)) * BYTES + ch * 16, src >= 0);
       }
     }
-    cp_async_wait<0>();
+    cp_async_commit();
+  };
+  // Uniform iterations k = -kRecAhead .. n-1, two commit groups each (empty when out of
+  // range).  Newest-first the pending groups before the first "wait<4>" are
+  //   [rec(k+4), gat(k+1), rec(k+3), gat(k), rec(k+2), ...]   -> rec(k+2) has landed
+  // and after issuing gat(k+2)
+  //   [gat(k+2), rec(k+4), gat(k+1), rec(k+3), gat(k), ...]   -> gat(k) has landed.
+  for (int k = -kRecAhead; k < n; ++k) {
+    issue_record(k + kRecAhead);
+    cp_async_wait<4>();
+    __syncwarp();
+    issue_gather(k + kGatherAhead);
+    cp_async_wait<4>();
+    __syncwarp();
+    if (k < 0) continue;
+    uint8_t* st = ring + (k % kStages) * STAGE;
+    const RecordInfo info = *reinterpret_cast<const RecordInfo*>(st + INFO);
+    const int32_t* trow = reinterpret_cast<const int32_t*>(st + INFO + 16);
+    if constexpr (EPI == EPI_PANEL) {  // density weights at the item's first tile
+      if (o.density && (info.flags & kRecFirst)) {
+        const int32_t r0 = trow[g], r1 = trow[g + 8];
+        wrow[0] = r0 >= 0 ? __ldg(o.density + r0) : 1.f;
+        wrow[1] = r1 >= 0 ? __ldg(o.density + r1) : 1.f;
+      }
+    }
+    uint32_t a[NCOMP][4], meta[NCOMP];
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c) {
+      // A rows of 32 B; the 16-B halves of row r are stored swapped when (r >> 2) & 1
+      const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
+      const int half = lane >> 4;
+      ldmatrix_x4(a[c], st + 128 + 576 * c + r * 32 + ((half ^ ((r >> 2) & 1)) * 16));
+      meta[c] = reinterpret_cast<const uint32_t*>(st + 640 + 576 * c)[g * 2 + (lane & 1)];
+    }
+    const uint8_t* B = st + REC;
+#pragma unroll
+    for (int nb = 0; nb < NB; ++nb) {
+      uint32_t b[4];
+      ldmatrix_x4_trans(b, B + lane * BYTES + chunk_swizzle<CH>(nb, lane) * 16);
+      const int ai = SPLIT ? (nb % NA) : nb;
+#pragma unroll
+      for (int c = 0; c < NCOMP; ++c) mma_sp_16832(acc[c][ai], a[c], b, meta[c]);
+    }
+    int32_t rows[2] = {-1, -1};
+    if (info.flags & kRecLast) {
+      rows[0] = trow[g];
+      rows[1] = trow[g + 8];
+    }
+    __syncwarp();  // stage k is reused by record(k + kStages) next iteration
+    if (info.flags & kRecLast) {  // last tile of its item
+      interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ>(acc, v, o, info, lane, rows, wrow, scale);
+#pragma unroll
+      for (int c = 0; c < NCOMP; ++c)
+#pragma unroll
+        for (int a2 = 0; a2 < NA; ++a2)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[c][a2][i] = 0.f;
+    }
   }
+  cp_async_wait<0>();
 }
 
 template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
 static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
   const int blocks = (v.n_warps + kInterpWarps - 1) / kInterpWarps;
-  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (128 + 576 * NCOMP + 32 * ROWH * 2);
+  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (record_bytes(NCOMP) + 32 * ROWH * 2);
   auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (blocks > 0) k<<<blocks, kInterpWarps * 32, smem, s>>>(v, panel, o);
@@ -323,7 +302,7 @@ static int sm_count();
 
 template <int ROWH, int NCOMP>
 static int resident_warps_t() {
-  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (128 + 576 * NCOMP + 32 * ROWH * 2);
+  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (record_bytes(NCOMP) + 32 * ROWH * 2);
   auto k = interp_mmasp_kernel<ROWH, true, NCOMP, EPI_GRID, NCOMP == 2>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   int per_sm = 0;

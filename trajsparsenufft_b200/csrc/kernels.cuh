@@ -26,36 +26,37 @@ struct CgState {
   int pad_;
 };
 
-// Interpolation view on the device: AoS tile records
-//   [0,128)            int32 col ids (internal panel row index)
-//   [128+576c, +512)   f16 compressed A of component c, [16][16]
-//   [640+576c, +64)    u32 mma.sp pair metadata of component c, [16]
+// Interpolation view on the device: AoS tile records, in the order the persistent warps
+// stream them (warp w owns records [warp_ranges[w].x, warp_ranges[w].y))
+//   [0,128)                  int32 gather row per column (internal panel row), -1 = dead
+//                            column (all coefficients zero: zero-filled, never read)
+//   [128+576c, +512)         f16 compressed A of component c, [16][16]
+//   [640+576c, +64)          u32 mma.sp pair metadata of component c, [16]
+//   [128+576n, +16)          RecordInfo (n = component count)
+//   [128+576n+16, +64)       int32 output row of each of the 16 tile rows, -1 pad
 // Work item: a run of at most kChunkTiles tiles of one 16-row group. Groups with more
 // tiles are split; their chunks write raw accumulators to `partials` and the warp that
 // arrives last (counter) sums all chunks in chunk order, so results stay deterministic.
 constexpr int kChunkTiles = 8;
-struct WorkItem {
-  int32_t group;
-  uint32_t t0, t1;
-  int32_t split;  // -1: whole group; else split-group id
+constexpr int kRecInfoBytes = 80;
+constexpr int kRecFirst = 1;  // first tile of a work item
+constexpr int kRecLast = 2;   // last tile of a work item: apply the epilogue
+struct RecordInfo {
+  int32_t flags;
+  int32_t split;       // -1: whole group; else split-group id (counter index)
+  int32_t first_slot;  // partials slot of chunk 0 of the split group
+  int32_t chunk;       // chunk index | nchunks << 16
 };
-struct SplitGroup {
-  int32_t first_slot;
-  int32_t nchunks;
-};
+static_assert(sizeof(RecordInfo) == 16, "record info is 16 bytes");
+__host__ __device__ constexpr int record_bytes(int ncomp) { return 128 + 576 * ncomp + kRecInfoBytes; }
 
 struct InterpView {
   const uint8_t* records = nullptr;
-  const uint32_t* group_offsets = nullptr;
-  const int32_t* group_rows = nullptr;  // internal row id, -1 pad
-  const WorkItem* items = nullptr;
-  const SplitGroup* splits = nullptr;
   int32_t* counters = nullptr;          // one per split group, zero between launches
   float* partials = nullptr;            // [slots][kPartialFloats][32]
-  const int2* warp_ranges = nullptr;    // per persistent warp: [first item, end item)
+  const int2* warp_ranges = nullptr;    // per persistent warp: [first record, end record)
   int32_t n_warps = 0;
   int32_t groups = 0;
-  int32_t n_items = 0;
   int32_t ncomp = 0;
   int32_t rec_bytes = 0;
 };

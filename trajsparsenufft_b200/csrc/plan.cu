@@ -69,7 +69,7 @@ struct HostView {
 };
 
 struct DevView {
-  DeviceBuffer records, offsets, rows, items, splits, counters, partials, ranges;
+  DeviceBuffer records, counters, partials, ranges;
   InterpView v;
   int64_t tiles = 0, groups = 0, active_rows = 0, nnz = 0, output_size = 0, n_cols = 0;
   bool present = false;
@@ -108,91 +108,116 @@ namespace {
 // reference cell index q0*G + q1 -> internal q1*G + q0
 inline int64_t cell_to_internal(int64_t q, int64_t g) { return (q % g) * g + q / g; }
 
+// Bit j set when column j of tile t has a nonzero coefficient in some row of some
+// component.  The others are the planner's padding (stored as column 0 in the pack files)
+// or columns whose entries all rounded to zero; the kernel zero-fills them instead of
+// gathering, which gives the same products for finite panels and keeps thousands of
+// gathers per launch off one panel row.
+uint32_t live_columns(const HostView& h, int64_t t) {
+  uint32_t m = 0;
+  for (size_t c = 0; c < h.a.size(); ++c) {
+    const uint32_t* pm = &h.meta[c][t * kMTile];
+    const uint16_t* a = &h.a[c][t * kMTile * (kKTile / 2)];
+    for (int r = 0; r < kMTile; ++r) {
+      // per-row 4-bit codes back from the mma.sp pair layout (rows g and g+8 share words)
+      const uint32_t lo = pm[2 * (r & 7)], hi = pm[2 * (r & 7) + 1];
+      const uint32_t word = r < 8 ? ((lo & 0xFFFFu) | ((hi & 0xFFFFu) << 16)) : ((lo >> 16) | (hi & 0xFFFF0000u));
+      for (int q = 0; q < kKTile / 4; ++q) {
+        const uint32_t code = (word >> (4 * q)) & 0xFu;
+        if (f16_bits_nonzero(a[r * (kKTile / 2) + 2 * q])) m |= 1u << (4 * q + (code & 3u));
+        if (f16_bits_nonzero(a[r * (kKTile / 2) + 2 * q + 1])) m |= 1u << (4 * q + ((code >> 2) & 3u));
+      }
+    }
+  }
+  return m;
+}
+
 void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
   DevView& d = P->view[which];
   const int64_t tiles = h.tiles(), groups = h.groups();
   const int ncomp = static_cast<int>(h.a.size());
-  const int rec = 128 + 576 * ncomp;
-  std::vector<uint8_t> records(static_cast<size_t>(tiles) * rec, 0);
-  for (int64_t t = 0; t < tiles; ++t) {
-    uint8_t* r = records.data() + t * rec;
-    int32_t cols[kKTile];
-    for (int j = 0; j < kKTile; ++j) {
-      int64_t c = h.tile_col_ids[t * kKTile + j];
-      if (cols_are_cells) c = cell_to_internal(c, P->G);
-      cols[j] = static_cast<int32_t>(c);
-    }
-    std::memcpy(r, cols, sizeof cols);
-    for (int c = 0; c < ncomp; ++c) {
-      // A: 16 rows of 32 B; the two 16-B halves of row r are swapped when (r >> 2) & 1 so
-      // ldmatrix reads 8 rows of one half without shared-memory bank conflicts
-      for (int row = 0; row < 16; ++row)
-        for (int half = 0; half < 2; ++half)
-          std::memcpy(r + 128 + 576 * c + row * 32 + ((half ^ ((row >> 2) & 1)) * 16),
-                      &h.a[c][t * 256 + row * 16 + half * 8], 16);
-      std::memcpy(r + 640 + 576 * c, &h.meta[c][t * 16], 64);
-    }
-  }
-  std::vector<int32_t> rows(h.group_row_ids.size());
-  for (size_t i = 0; i < rows.size(); ++i) {
-    const int32_t v = h.group_row_ids[i];
-    rows[i] = (v >= 0 && rows_are_cells) ? static_cast<int32_t>(cell_to_internal(v, P->G)) : v;
-  }
+  const int rec = record_bytes(ncomp);
   // work items: groups of at most kChunkTiles tiles run whole; longer groups are split into
   // chunks (scheduled first, they are the long poles) reduced in chunk order
-  std::vector<WorkItem> big, small;
-  std::vector<SplitGroup> splits;
-  int32_t slots = 0;
+  struct Item {
+    int32_t group;
+    uint32_t t0, t1;
+    int32_t split, first_slot, chunk, nchunks;
+  };
+  std::vector<Item> items, small;
+  int32_t slots = 0, nsplit = 0;
   for (int64_t g = 0; g < groups; ++g) {
     const uint32_t a = h.group_offsets[g], b = h.group_offsets[g + 1];
+    if (a == b) continue;  // no tiles: nothing to stream (grid rows stay zero)
     if (b - a <= static_cast<uint32_t>(kChunkTiles)) {
-      small.push_back(WorkItem{static_cast<int32_t>(g), a, b, -1});
+      small.push_back(Item{static_cast<int32_t>(g), a, b, -1, 0, 0, 1});
       continue;
     }
     const int32_t nch = static_cast<int32_t>((b - a + kChunkTiles - 1) / kChunkTiles);
-    const int32_t sid = static_cast<int32_t>(splits.size());
-    splits.push_back(SplitGroup{slots, nch});
-    slots += nch;
+    if (nch >= (1 << 15)) fail(TSN_ERR_UNSUPPORTED, "a row group has too many tiles");
     for (int32_t k = 0; k < nch; ++k)
-      big.push_back(WorkItem{static_cast<int32_t>(g), a + k * kChunkTiles,
-                             std::min<uint32_t>(b, a + (k + 1) * kChunkTiles), sid});
+      items.push_back(Item{static_cast<int32_t>(g), a + k * kChunkTiles,
+                           std::min<uint32_t>(b, a + (k + 1) * kChunkTiles), nsplit, slots, k, nch});
+    slots += nch;
+    ++nsplit;
   }
-  big.insert(big.end(), small.begin(), small.end());
-  // persistent warps: contiguous runs of items with about the same number of tiles each
+  items.insert(items.end(), small.begin(), small.end());
+  // persistent warps: contiguous runs of items with about the same number of tiles each;
+  // records are stored in that stream order so each warp reads one contiguous range
   const int resident = interp_resident_warps(4 * P->C, ncomp);
-  int64_t total_tiles = 0;
-  for (const WorkItem& w : big) total_tiles += w.t1 - w.t0;
-  const int64_t target = std::max<int64_t>(1, (total_tiles + resident - 1) / resident);
+  const int64_t target = std::max<int64_t>(1, (tiles + resident - 1) / resident);
   std::vector<int2> ranges;
-  int64_t acc_tiles = 0;
-  int first = 0;
-  for (int i = 0; i < static_cast<int>(big.size()); ++i) {
-    acc_tiles += big[i].t1 - big[i].t0;
-    if (acc_tiles >= target) {
-      ranges.push_back(make_int2(first, i + 1));
-      first = i + 1;
-      acc_tiles = 0;
+  std::vector<uint8_t> records(static_cast<size_t>(tiles) * rec, 0);
+  int64_t pos = 0, run_start = 0;
+  for (const Item& it : items) {
+    for (uint32_t t = it.t0; t < it.t1; ++t, ++pos) {
+      uint8_t* r = records.data() + pos * rec;
+      const uint32_t live = live_columns(h, t);
+      int32_t cols[kKTile];
+      for (int j = 0; j < kKTile; ++j) {
+        int64_t c = h.tile_col_ids[t * kKTile + j];
+        if (cols_are_cells) c = cell_to_internal(c, P->G);
+        cols[j] = ((live >> j) & 1u) ? static_cast<int32_t>(c) : -1;
+      }
+      std::memcpy(r, cols, sizeof cols);
+      for (int c = 0; c < ncomp; ++c) {
+        // A: 16 rows of 32 B; the two 16-B halves of row r are swapped when (r >> 2) & 1 so
+        // ldmatrix reads 8 rows of one half without shared-memory bank conflicts
+        for (int row = 0; row < 16; ++row)
+          for (int half = 0; half < 2; ++half)
+            std::memcpy(r + 128 + 576 * c + row * 32 + ((half ^ ((row >> 2) & 1)) * 16),
+                        &h.a[c][t * 256 + row * 16 + half * 8], 16);
+        std::memcpy(r + 640 + 576 * c, &h.meta[c][t * 16], 64);
+      }
+      RecordInfo info;
+      info.flags = (t == it.t0 ? kRecFirst : 0) | (t + 1 == it.t1 ? kRecLast : 0);
+      info.split = it.split;
+      info.first_slot = it.first_slot;
+      info.chunk = it.chunk | (it.nchunks << 16);
+      std::memcpy(r + 128 + 576 * ncomp, &info, sizeof info);
+      int32_t orow[kMTile];
+      for (int s = 0; s < kMTile; ++s) {
+        const int32_t v = h.group_row_ids[static_cast<size_t>(it.group) * kMTile + s];
+        orow[s] = (v >= 0 && rows_are_cells) ? static_cast<int32_t>(cell_to_internal(v, P->G)) : v;
+      }
+      std::memcpy(r + 128 + 576 * ncomp + sizeof info, orow, sizeof orow);
+    }
+    if (pos - run_start >= target) {
+      ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(pos)));
+      run_start = pos;
     }
   }
-  if (first < static_cast<int>(big.size())) ranges.push_back(make_int2(first, static_cast<int>(big.size())));
+  if (pos != tiles) fail(TSN_ERR_FORMAT, "group offsets do not cover the tiles");
+  if (run_start < pos) ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(pos)));
   d.records.upload(records);
-  d.offsets.upload(h.group_offsets);
-  d.rows.upload(rows);
-  d.items.upload(big);
-  d.splits.upload(splits);
-  d.counters.upload(std::vector<int32_t>(std::max<size_t>(splits.size(), 1), 0));
+  d.counters.upload(std::vector<int32_t>(std::max(nsplit, 1), 0));
   d.partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kPartialFloats * 32);
-  d.v.items = d.items.as<WorkItem>();
-  d.v.splits = d.splits.as<SplitGroup>();
+  d.ranges.upload(ranges);
+  d.v.records = d.records.as<uint8_t>();
   d.v.counters = d.counters.as<int32_t>();
   d.v.partials = d.partials.as<float>();
-  d.v.n_items = static_cast<int32_t>(big.size());
-  d.ranges.upload(ranges);
   d.v.warp_ranges = d.ranges.as<int2>();
   d.v.n_warps = static_cast<int32_t>(ranges.size());
-  d.v.records = d.records.as<uint8_t>();
-  d.v.group_offsets = d.offsets.as<uint32_t>();
-  d.v.group_rows = d.rows.as<int32_t>();
   d.v.groups = static_cast<int32_t>(groups);
   d.v.ncomp = ncomp;
   d.v.rec_bytes = rec;
@@ -207,7 +232,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   P->info.tiles[which] = tiles;
   P->info.active_rows[which] = h.active_rows;
   P->info.nnz[which] = h.nnz;
-  P->info.pack_bytes[which] = static_cast<int64_t>(records.size() + h.group_offsets.size() * 4 + rows.size() * 4);
+  P->info.pack_bytes[which] = static_cast<int64_t>(records.size());
 }
 
 void check_desc(const tsn_plan_desc* d) {
@@ -798,20 +823,24 @@ tsn_status tsn_interp_component(tsn_plan* plan, int32_t view, int32_t component,
     InterpOut o;
     o.raw = dout.as<float>();
     o.rows = d.output_size;
-    // component selection: records of component c start 576*c bytes later for A/meta
+    // component selection: a two-component view gets a single-component record copy
+    // (columns | A and metadata of the component | record info and rows)
     DeviceBuffer shifted;
-    if (component != 0) {
-      // build a single-component record copy for component 1
+    if (d.v.ncomp == 2) {
+      const int one_rec = record_bytes(1);
       std::vector<uint8_t> host(static_cast<size_t>(d.tiles) * d.v.rec_bytes);
       CUDA_OK(cudaMemcpy(host.data(), d.v.records, host.size(), cudaMemcpyDeviceToHost));
-      std::vector<uint8_t> one(static_cast<size_t>(d.tiles) * 704);
+      std::vector<uint8_t> one(static_cast<size_t>(d.tiles) * one_rec);
       for (int64_t t = 0; t < d.tiles; ++t) {
-        std::memcpy(&one[t * 704], &host[t * d.v.rec_bytes], 128);
-        std::memcpy(&one[t * 704 + 128], &host[t * d.v.rec_bytes + 128 + 576], 576);
+        const uint8_t* src = &host[t * d.v.rec_bytes];
+        uint8_t* dst = &one[t * one_rec];
+        std::memcpy(dst, src, 128);
+        std::memcpy(dst + 128, src + 128 + 576 * component, 576);
+        std::memcpy(dst + 128 + 576, src + 128 + 576 * 2, kRecInfoBytes);
       }
       shifted.upload(one);
       v.records = shifted.as<uint8_t>();
-      v.rec_bytes = 704;
+      v.rec_bytes = one_rec;
     }
     v.ncomp = 1;
     launch_interp(v, din.as<__half>(), 16, false, EPI_RAW, false, o, s);
