@@ -41,7 +41,8 @@ def test_forward_panel_matches_numpy_fft(name, layout):
     assert rel_l2(got, want) <= 1e-5
 
 
-@pytest.mark.parametrize("name,layout", [("small", "centered"), ("cfg0", "reference"), ("headline", "centered")])
+@pytest.mark.parametrize("name,layout", [("small", "centered"), ("cfg0", "reference"), ("headline", "centered"),
+                                         ("c16", "centered")])
 def test_adjoint_endpoint_matches_numpy_ifft(name, layout):
     from trajsparsenufft_b200.operator import Plan
     traj, x, s, n, g, c, j, _ = case(name)

@@ -144,3 +144,20 @@ def test_cg_curvature_failure_is_reported_not_trapped():
     x, hist, status = plan.cg_sense(yt, st, lam=-1e12, iters=3)
     assert status["positive_curvature"] is False
     assert status.get("failure") == "CURVATURE"
+
+
+def test_misaligned_device_arrays_are_rejected():
+    """The FFT stages stream images and maps with 16-byte copies: an array that starts
+    8 bytes into an allocation is refused with an argument error before any launch."""
+    from trajsparsenufft_b200._lib import TsnError
+    plan = _plan("small")
+    xt, st, yt = torch_inputs("small")
+    n = plan.im_size
+    buf = torch.zeros(n * n + 1, dtype=torch.complex64, device="cuda")
+    x_off = buf[1:].view(n, n)
+    assert x_off.data_ptr() % 16 == 8
+    with pytest.raises(TsnError, match="16-byte aligned") as info:
+        plan.forward(x_off, st)
+    assert info.value.kind == "ARG"
+    y = plan.forward(xt, st)  # the plan stays usable
+    assert torch.isfinite(torch.view_as_real(y)).all()

@@ -11,6 +11,7 @@
 // the coil-major grids of nufft_custom_fft_forward_bench.cu:538-747; here every stage
 // reads and writes contiguous slabs and the panel row carries hi and res together so one
 // gather feeds both sparse MMAs.
+#include <algorithm>
 #include <cstdio>
 #include <vector>
 #include <cmath>
@@ -372,10 +373,6 @@ struct FftSmem {
   static constexpr int SCR = WarpFftShape<G>::SCRATCH;
 };
 
-__device__ __forceinline__ void load_twiddles(float2* tw_s, const float2* tw, int G) {
-  for (int i = threadIdx.x; i < G; i += blockDim.x) tw_s[i] = tw[i];
-}
-
 // Copy `bytes` (multiple of 16) from global to shared with 16-byte cp.async, all threads.
 __device__ __forceinline__ void cp_async_bytes(void* dst, const void* src, int bytes) {
   uint8_t* d = static_cast<uint8_t*>(dst);
@@ -401,33 +398,57 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
   }
 }
 
-// The four FFT stages are persistent CTAs (one warp per coil) walking their items with a
-// double-buffered cp.async input slab: item i+1 streams in while item i is transformed.
+// The four FFT stages run one warp per coil in CTAs of 32*C threads (C <= MAXW). With
+// MAXW = 8 and G <= 512 the 80-register cap keeps three CTAs resident per SM. The per-warp
+// FFT scratch and the output staging reuse the input slab's shared memory once it is
+// consumed, which keeps a CTA near 72 KB. The column stages double-buffer the slab when two
+// regions fit, so the next item streams in while the current one is transformed.
+#define TSN_FFT_BOUNDS(G, MAXW) __launch_bounds__((MAXW) * 32, ((MAXW) <= 8 && (G) <= 512) ? 3 : 1)
 
 // Forward rows (x-stage). Image row i0 -> z1[q1][i0][c] for all q1. Fuses the SENSE
 // multiply, deapodization, power-of-two panel scaling, zero-padding and (CG) p = r + beta p.
-// Input slab per row: [row0 N][row1 N][maps C*N] float2 + [scaling N] float
-//   mode 0 with smaps:  row0 = x row, maps = S_c rows      (row1 unused)
-//   mode 0 without:     maps = coil-image rows
-//   mode 1 (CG):        row0 = r row, row1 = p row, maps = S_c rows
+// Shared memory: twiddles [G] | one region that holds, in turn,
+//   the input slab  [row0 N][row1 N][maps C*N] float2 + [scaling N] float
+//     mode 0 with smaps:  row0 = x row, maps = S_c rows      (row1 unused)
+//     mode 0 without:     maps = coil-image rows
+//     mode 1 (CG):        row0 = r row, row1 = p row, maps = S_c rows
+//   the per-warp FFT scratch [C][SCR], and the output rows [G][C+1] float2.
 // Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844).
-template <int G>
-__global__ void __launch_bounds__(512) fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1,
-                                                       int mode, float2* __restrict__ p, const float2* __restrict__ r,
-                                                       const double* __restrict__ parts, int nparts,
-                                                       CgState* __restrict__ st, int iter) {
+template <int G, int MAXW>
+__global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1,
+                                                     int mode, float2* __restrict__ p, const float2* __restrict__ r,
+                                                     const double* __restrict__ parts, int nparts,
+                                                     CgState* __restrict__ st, int iter) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N, C = f.C;
-  const int in_f2 = (2 + C) * N;                         // float2 per slab (+ N floats of scaling)
-  const int in_bytes = in_f2 * 8 + N * 4;
+  const int in_f2 = (2 + C) * N;  // float2 of the slab before the scaling row
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  uint8_t* inb = reinterpret_cast<uint8_t*>(tw_s + G);   // [2][in_bytes]
-  float2* out_s = reinterpret_cast<float2*>(inb + 2 * in_bytes);  // [G][C+1] (padded)
-  float2* scr = out_s + G * (C + 1);                     // [C][SCR]
+  uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
+  float2* row0 = reinterpret_cast<float2*>(reg);
+  float2* row1 = row0 + N;
+  float2* maps = row1 + N;
+  const float* srow = reinterpret_cast<const float*>(reg + in_f2 * 8);
+  float2* scr = reinterpret_cast<float2*>(reg);
+  float2* out_s = reinterpret_cast<float2*>(reg);  // [G][C+1]
   __shared__ double red[33];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  load_twiddles(tw_s, f.tw, G);
+  auto issue = [&](int i0) {
+    const size_t off = static_cast<size_t>(i0) * N;
+    if (mode == 1) {
+      cp_async_bytes(row0, r + off, N * 8);
+      if (iter > 0) cp_async_bytes(row1, p + off, N * 8);
+    } else if (f.smaps) {
+      cp_async_bytes(row0, x + off, N * 8);
+    }
+    const float2* msrc = f.smaps ? f.smaps : x;
+    for (int c = 0; c < C; ++c) cp_async_bytes(maps + c * N, msrc + static_cast<size_t>(c) * N * N + off, N * 8);
+    cp_async_bytes(reg + in_f2 * 8, f.scaling + off, N * 4);
+    cp_async_commit();
+  };
+  // the first item (and the twiddles) stream in while the panel scale is reduced
+  cp_async_bytes(tw_s, f.tw, G * 8);
+  if (blockIdx.x < N) issue(blockIdx.x);
   const double total = sum_partials(parts, nparts, red);
   float sigma;
   double beta = 0.0;
@@ -445,39 +466,16 @@ __global__ void __launch_bounds__(512) fwd_rows_kernel(FftArgs f, const float2* 
   }
   const float bf = static_cast<float>(beta);
   const float scl = sigma / static_cast<float>(G);
-  auto prefetch = [&](int i0, int buf) {
-    uint8_t* dst = inb + buf * in_bytes;
-    float2* row0 = reinterpret_cast<float2*>(dst);
-    float2* row1 = row0 + N;
-    float2* maps = row1 + N;
-    const size_t off = static_cast<size_t>(i0) * N;
-    if (mode == 1) {
-      cp_async_bytes(row0, r + off, N * 8);
-      if (iter > 0) cp_async_bytes(row1, p + off, N * 8);
-    } else if (f.smaps) {
-      cp_async_bytes(row0, x + off, N * 8);
+  // output copy: C/2 16-byte chunks per grid row, 64 rows per pass of the 32*C threads
+  const int ch2 = C >> 1;
+  const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
+  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x) {
+    if (i0 != blockIdx.x) {
+      __syncthreads();  // the previous item's output rows are copied out
+      issue(i0);
     }
-    const float2* msrc = f.smaps ? f.smaps : x;
-    for (int c = 0; c < C; ++c) cp_async_bytes(maps + c * N, msrc + static_cast<size_t>(c) * N * N + off, N * 8);
-    cp_async_bytes(dst + in_f2 * 8, f.scaling + off, N * 4);
-    cp_async_commit();
-  };
-  int buf = 0;
-  if (blockIdx.x < N) prefetch(blockIdx.x, 0);
-  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x, buf ^= 1) {
-    const int next = i0 + gridDim.x;
-    if (next < N) {
-      prefetch(next, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    cp_async_wait<0>();
     __syncthreads();
-    uint8_t* in = inb + buf * in_bytes;
-    float2* row0 = reinterpret_cast<float2*>(in);
-    const float2* row1 = row0 + N;
-    const float2* maps = row1 + N;
-    const float* srow = reinterpret_cast<const float*>(in + in_f2 * 8);
     if (mode == 1) {  // p = r + beta p (p = r at iteration 0); row0 becomes p
       for (int i = threadIdx.x; i < N; i += blockDim.x) {
         float2 pv = row0[i];
@@ -490,90 +488,94 @@ __global__ void __launch_bounds__(512) fwd_rows_kernel(FftArgs f, const float2* 
       }
       __syncthreads();
     }
-    if (warp < C) {
-      const int c = warp;
-      float2 v[P];
+    float2 v[P];
+    const int c = warp;
 #pragma unroll
-      for (int j = 0; j < P; ++j) {
-        const int n = lane + 32 * j;
-        int i1 = n + f.shift;
-        if (i1 >= G) i1 -= G;
-        float2 val = make_float2(0.f, 0.f);
-        if (i1 < N) {
-          const float d = srow[i1] * scl;
-          val = (f.smaps || mode == 1) ? cscale(cmul(row0[i1], maps[c * N + i1]), d) : cscale(maps[c * N + i1], d);
-        }
-        v[j] = val;
+    for (int j = 0; j < P; ++j) {
+      const int n = lane + 32 * j;
+      int i1 = n + f.shift;
+      if (i1 >= G) i1 -= G;
+      float2 val = make_float2(0.f, 0.f);
+      if (i1 < N) {
+        const float d = srow[i1] * scl;
+        val = (f.smaps || mode == 1) ? cscale(cmul(row0[i1], maps[c * N + i1]), d) : cscale(maps[c * N + i1], d);
       }
-      warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
-#pragma unroll
-      for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * (C + 1) + c] = v[m];
+      v[j] = val;
     }
+    __syncthreads();  // slab consumed: the region becomes FFT scratch
+    warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();  // scratch free: the region becomes the output rows
+#pragma unroll
+    for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * (C + 1) + c] = v[m];
     __syncthreads();
-    for (int e = threadIdx.x; e < G * C; e += blockDim.x) {
-      const int q1 = e / C, c = e - q1 * C;
-      z1[(static_cast<size_t>(q1) * N + i0) * C + c] = out_s[q1 * (C + 1) + c];
+    for (int q1 = crow; q1 < G; q1 += 64) {
+      const float2 a = out_s[q1 * (C + 1) + 2 * ck], b = out_s[q1 * (C + 1) + 2 * ck + 1];
+      *reinterpret_cast<float4*>(z1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * ck) = make_float4(a.x, a.y, b.x, b.y);
     }
   }
 }
 
 // Forward columns (y-stage): z1[q1][*][c] -> panel rows q1*G + q0, FP16 hi | res.
+// Shared memory: twiddles [G] | nbuf regions of `region` bytes, each holding in turn the
+// swizzled input slab [N][C], the per-warp FFT scratch and the output rows [G][2C+1] words.
 // Reference: fft512_allcoils1_shared16_to_n16 (nufft_custom_fft_forward_bench.cu:538-747).
-template <int G>
-__global__ void __launch_bounds__(512) fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1,
-                                                       __half* __restrict__ panel) {
+template <int G, int MAXW>
+__global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1,
+                                                     __half* __restrict__ panel, int region, int nbuf) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* inb = tw_s + G;                              // [2][N*C]
-  float2* scr = inb + 2 * N * C;                       // [C][SCR]
-  uint32_t* out_s = reinterpret_cast<uint32_t*>(scr + C * FftSmem<G>::SCR);  // [G][2C+1] half2 (padded)
+  uint8_t* regs = reinterpret_cast<uint8_t*>(tw_s + G);
   const int OP = 2 * C + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  load_twiddles(tw_s, f.tw, G);
-  auto prefetch = [&](int q1, int buf) {
-    cp_async_slab(inb + buf * N * C, z1 + static_cast<size_t>(q1) * N * C, N, C);
+  auto issue = [&](int q1, int b) {
+    cp_async_slab(reinterpret_cast<float2*>(regs + b * region), z1 + static_cast<size_t>(q1) * N * C, N, C);
     cp_async_commit();
   };
-  int buf = 0;
-  if (blockIdx.x < G) prefetch(blockIdx.x, 0);
-  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, buf ^= 1) {
-    const int next = q1 + gridDim.x;
-    if (next < G) {
-      prefetch(next, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  cp_async_bytes(tw_s, f.tw, G * 8);
+  if (blockIdx.x < G) issue(blockIdx.x, 0);
+  const int ch2 = C >> 1;  // 16-byte chunks per panel row
+  const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
+  const int c = warp;
+  int it = 0;
+  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, ++it) {
+    const int b = nbuf == 2 ? (it & 1) : 0;
+    if (nbuf == 1 && it > 0) {
+      __syncthreads();  // the previous item's output rows are copied out
+      issue(q1, 0);
     }
+    cp_async_wait<0>();
     __syncthreads();
-    const float2* in_s = inb + buf * N * C;
-    if (warp < C) {
-      const int c = warp;
-      float2 v[P];
+    if (nbuf == 2 && q1 + gridDim.x < G) issue(q1 + gridDim.x, b ^ 1);
+    uint8_t* reg = regs + b * region;
+    const float2* in_s = reinterpret_cast<const float2*>(reg);
+    float2 v[P];
 #pragma unroll
-      for (int j = 0; j < P; ++j) {
-        const int n = lane + 32 * j;
-        int i0 = n + f.shift;
-        if (i0 >= G) i0 -= G;
-        v[j] = i0 < N ? in_s[slab_idx(i0, c, C)] : make_float2(0.f, 0.f);
-      }
-      warp_fft<G, false>(v, scr + c * FftSmem<G>::SCR, tw_s);
+    for (int j = 0; j < P; ++j) {
+      const int n = lane + 32 * j;
+      int i0 = n + f.shift;
+      if (i0 >= G) i0 -= G;
+      v[j] = i0 < N ? in_s[slab_idx(i0, c, C)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();  // slab consumed
+    warp_fft<G, false>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();  // scratch free
+    uint32_t* out_s = reinterpret_cast<uint32_t*>(reg);
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        const int q0 = warp_fft_out_index<G>(m);
-        __half hr, rr, hi, ri;
-        split_hi_res(v[m].x, hr, rr);
-        split_hi_res(v[m].y, hi, ri);
-        out_s[q0 * OP + c] = pack_half2(hr, hi);
-        out_s[q0 * OP + C + c] = pack_half2(rr, ri);
-      }
+    for (int m = 0; m < P; ++m) {
+      const int q0 = warp_fft_out_index<G>(m);
+      __half hr, rr, hi, ri;
+      split_hi_res(v[m].x, hr, rr);
+      split_hi_res(v[m].y, hi, ri);
+      out_s[q0 * OP + c] = pack_half2(hr, hi);
+      out_s[q0 * OP + C + c] = pack_half2(rr, ri);
     }
     __syncthreads();
     uint32_t* dst = reinterpret_cast<uint32_t*>(panel + static_cast<size_t>(q1) * G * 4 * C);
-    for (int i = threadIdx.x; i < G * 2 * C; i += blockDim.x) {
-      const int q0 = i / (2 * C), w = i - q0 * 2 * C;
-      dst[i] = out_s[q0 * OP + w];
+    for (int q0 = crow; q0 < G; q0 += 64) {
+      const uint32_t* s = out_s + q0 * OP + 4 * ck;
+      *reinterpret_cast<uint4*>(dst + q0 * 2 * C + 4 * ck) = make_uint4(s[0], s[1], s[2], s[3]);
     }
   }
 }
@@ -615,126 +617,142 @@ __global__ void split_samples_kernel(const float2* __restrict__ y, const float* 
 }
 
 // Inverse columns: grid rows q1*G + [0,G) (all coils) -> w1[q1][i0][c], i0 < N (crop).
+// Shared memory: twiddles [G] | nbuf regions, each holding in turn the swizzled slab [G][C],
+// the per-warp FFT scratch and the cropped output rows [N][C+1] float2.
 // Reference: ifft512_rows8_regular_transposed (nufft_custom_fft_forward_bench.cu:1463-1515).
-template <int G>
-__global__ void __launch_bounds__(512) inv_cols_kernel(FftArgs f, const float2* __restrict__ grid,
-                                                       float2* __restrict__ w1) {
+template <int G, int MAXW>
+__global__ void TSN_FFT_BOUNDS(G, MAXW) inv_cols_kernel(FftArgs f, const float2* __restrict__ grid,
+                                                     float2* __restrict__ w1, int region, int nbuf) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* inb = tw_s + G;                // [2][G*C] swizzled slabs
-  float2* out_s = inb + 2 * G * C;       // [N][C+1] (padded)
-  float2* scr = out_s + N * (C + 1);     // [C][SCR]
+  uint8_t* regs = reinterpret_cast<uint8_t*>(tw_s + G);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  load_twiddles(tw_s, f.tw, G);
-  auto prefetch = [&](int q1, int buf) {
-    cp_async_slab(inb + buf * G * C, grid + static_cast<size_t>(q1) * G * C, G, C);
+  auto issue = [&](int q1, int b) {
+    cp_async_slab(reinterpret_cast<float2*>(regs + b * region), grid + static_cast<size_t>(q1) * G * C, G, C);
     cp_async_commit();
   };
-  int buf = 0;
-  if (blockIdx.x < G) prefetch(blockIdx.x, 0);
-  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, buf ^= 1) {
-    const int next = q1 + gridDim.x;
-    if (next < G) {
-      prefetch(next, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  cp_async_bytes(tw_s, f.tw, G * 8);
+  if (blockIdx.x < G) issue(blockIdx.x, 0);
+  const int ch2 = C >> 1;  // 16-byte chunks per output row
+  const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
+  const int c = warp;
+  int it = 0;
+  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, ++it) {
+    const int b = nbuf == 2 ? (it & 1) : 0;
+    if (nbuf == 1 && it > 0) {
+      __syncthreads();
+      issue(q1, 0);
     }
+    cp_async_wait<0>();
     __syncthreads();
-    const float2* in_s = inb + buf * G * C;
-    if (warp < C) {
-      const int c = warp;
-      float2 v[P];
+    if (nbuf == 2 && q1 + gridDim.x < G) issue(q1 + gridDim.x, b ^ 1);
+    uint8_t* reg = regs + b * region;
+    const float2* in_s = reinterpret_cast<const float2*>(reg);
+    float2 v[P];
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
-      warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
+    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
+    __syncthreads();
+    warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();
+    float2* out_s = reinterpret_cast<float2*>(reg);  // [N][C+1]
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        int i0 = warp_fft_out_index<G>(m) + f.shift;
-        if (i0 >= G) i0 -= G;
-        if (i0 < N) out_s[i0 * (C + 1) + c] = v[m];
-      }
+    for (int m = 0; m < P; ++m) {
+      int i0 = warp_fft_out_index<G>(m) + f.shift;
+      if (i0 >= G) i0 -= G;
+      if (i0 < N) out_s[i0 * (C + 1) + c] = v[m];
     }
     __syncthreads();
     float2* dst = w1 + static_cast<size_t>(q1) * N * C;
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
-      const int i0 = i / C, c = i - i0 * C;
-      dst[i] = out_s[i0 * (C + 1) + c];
+    for (int i0 = crow; i0 < N; i0 += 64) {
+      const float2 a = out_s[i0 * (C + 1) + 2 * ck], bb = out_s[i0 * (C + 1) + 2 * ck + 1];
+      *reinterpret_cast<float4*>(dst + i0 * C + 2 * ck) = make_float4(a.x, a.y, bb.x, bb.y);
     }
   }
 }
 
 // Inverse rows + crop + deapodization + SENSE coil combine (+ CG epilogues).
+// Shared memory: twiddles [G] | a region holding in turn the swizzled slab [G][C], the
+// per-warp FFT scratch and the coil images [C][N] | (epi_smem) the epilogue inputs of the
+// row, fetched in the slab's copy group: maps [C][N] (with smaps), p row [N] (mode 2),
+// scaling row [N] float. Without epi_smem the epilogue reads them from global memory.
 // Reference: ifft512_rows8_regular_crop_scale (nufft_custom_fft_forward_bench.cu:1517-1552)
 // followed by sense_combine_scaled (nufft_fp16x2_cg_bench.cu:27-54).
-template <int G>
-__global__ void __launch_bounds__(512) inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2* __restrict__ out,
-                                                       int mode, float2* __restrict__ x, float2* __restrict__ r,
-                                                       const float2* __restrict__ p, double* __restrict__ parts,
-                                                       CgState* __restrict__ st, int iter, float inv_scale2,
-                                                       float lambda_scaled) {
+template <int G, int MAXW>
+__global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2* __restrict__ out,
+                                                     int mode, float2* __restrict__ x, float2* __restrict__ r,
+                                                     const float2* __restrict__ p, double* __restrict__ parts,
+                                                     CgState* __restrict__ st, int iter, float inv_scale2,
+                                                     float lambda_scaled, int region, int epi_smem) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N, C = f.C;
   float2* tw_s = reinterpret_cast<float2*>(sm);
-  float2* inb = tw_s + G;                // [2][G*C]
-  float2* img_s = inb + 2 * G * C;       // [C][N]
-  float2* scr = img_s + N * C;           // [C][SCR]
+  uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
+  float2* emaps = reinterpret_cast<float2*>(reg + region);
+  float2* eprow = emaps + (f.smaps ? C * N : 0);
+  float* escale = reinterpret_cast<float*>(eprow + (mode == 2 ? N : 0));
   __shared__ double red[33];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  load_twiddles(tw_s, f.tw, G);
-  float factor;
-  if (mode == 2) factor = static_cast<float>(G) / st->sigma[iter] * inv_scale2;
-  else factor = inv_scale2 / st->sigma_y;
-  auto prefetch = [&](int i0, int buf) {
-    float2* dst = inb + buf * G * C;
+  auto issue = [&](int i0) {
+    float2* dst = reinterpret_cast<float2*>(reg);
     // G runs of C complex values (8C bytes each, 16-byte aligned for even C), swizzled
     const int chn = C / 2;
     for (int e = threadIdx.x; e < G * chn; e += blockDim.x) {
       const int q1 = e / chn, k = e - q1 * chn;
       cp_async16(dst + q1 * C + 2 * (k ^ slab_swz(q1, chn)), w1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * k);
     }
+    if (epi_smem) {
+      const size_t off = static_cast<size_t>(i0) * N;
+      if (f.smaps)
+        for (int c = 0; c < C; ++c) cp_async_bytes(emaps + c * N, f.smaps + static_cast<size_t>(c) * N * N + off, N * 8);
+      if (mode == 2) cp_async_bytes(eprow, p + off, N * 8);
+      cp_async_bytes(escale, f.scaling + off, N * 4);
+    }
     cp_async_commit();
   };
-  int buf = 0;
-  if (blockIdx.x < N) prefetch(blockIdx.x, 0);
-  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x, buf ^= 1) {
-    const int next = i0 + gridDim.x;
-    if (next < N) {
-      prefetch(next, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  cp_async_bytes(tw_s, f.tw, G * 8);
+  if (blockIdx.x < N) issue(blockIdx.x);
+  float factor;
+  if (mode == 2) factor = static_cast<float>(G) / st->sigma[iter] * inv_scale2;
+  else factor = inv_scale2 / st->sigma_y;
+  const int c = warp;
+  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x) {
+    if (i0 != blockIdx.x) {
+      __syncthreads();
+      issue(i0);
     }
+    cp_async_wait<0>();
     __syncthreads();
-    const float2* in_s = inb + buf * G * C;
-    if (warp < C) {
-      const int c = warp;
-      float2 v[P];
+    const float2* in_s = reinterpret_cast<const float2*>(reg);
+    float2 v[P];
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
-      warp_fft<G, true>(v, scr + c * FftSmem<G>::SCR, tw_s);
+    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
+    __syncthreads();
+    warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();
+    float2* img_s = reinterpret_cast<float2*>(reg);  // [C][N]
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        int i1 = warp_fft_out_index<G>(m) + f.shift;
-        if (i1 >= G) i1 -= G;
-        if (i1 < N) img_s[c * N + i1] = v[m];
-      }
+    for (int m = 0; m < P; ++m) {
+      int i1 = warp_fft_out_index<G>(m) + f.shift;
+      if (i1 >= G) i1 -= G;
+      if (i1 < N) img_s[c * N + i1] = v[m];
     }
     __syncthreads();
     double dot = 0.0;
     for (int i1 = threadIdx.x; i1 < N; i1 += blockDim.x) {
       const size_t pix = static_cast<size_t>(i0) * N + i1;
-      const float d = f.scaling[pix] * factor;
+      const float d = (epi_smem ? escale[i1] : f.scaling[pix]) * factor;
       if (!f.smaps) {  // coil images out [C][N][N]
-        for (int c = 0; c < C; ++c) out[static_cast<size_t>(c) * N * N + pix] = cscale(img_s[c * N + i1], d);
+        for (int cc = 0; cc < C; ++cc) out[static_cast<size_t>(cc) * N * N + pix] = cscale(img_s[cc * N + i1], d);
         continue;
       }
       float2 acc = make_float2(0.f, 0.f);
-      for (int c = 0; c < C; ++c)
-        acc = cadd(acc, cmulc(img_s[c * N + i1], f.smaps[static_cast<size_t>(c) * N * N + pix]));
+      for (int cc = 0; cc < C; ++cc) {
+        const float2 s = epi_smem ? emaps[cc * N + i1] : f.smaps[static_cast<size_t>(cc) * N * N + pix];
+        acc = cadd(acc, cmulc(img_s[cc * N + i1], s));
+      }
       acc = cscale(acc, d);
       if (mode == 0) {
         out[pix] = acc;
@@ -743,7 +761,7 @@ __global__ void __launch_bounds__(512) inv_rows_kernel(FftArgs f, const float2* 
         x[pix] = make_float2(0.f, 0.f);
         dot += static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y;
       } else {
-        const float2 pv = p[pix];
+        const float2 pv = epi_smem ? eprow[i1] : p[pix];
         acc.x += lambda_scaled * pv.x;
         acc.y += lambda_scaled * pv.y;
         out[pix] = acc;
@@ -803,25 +821,42 @@ __global__ void cg_finish_kernel(int N, const double* __restrict__ rr_parts, CgS
 // ------------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------------
+constexpr size_t kFftTwoCtaSmem = 114 * 1024;  // at most this per CTA keeps two CTAs per SM
+
+static size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
+
 template <int G>
-static size_t fwd_rows_smem(const FftArgs& f) {
-  const size_t in_bytes = static_cast<size_t>(2 + f.C) * f.N * 8 + static_cast<size_t>(f.N) * 4;
-  return sizeof(float2) * G + 2 * in_bytes +
-         sizeof(float2) * (static_cast<size_t>(G) * (f.C + 1) + static_cast<size_t>(f.C) * FftSmem<G>::SCR);
+static size_t fft_scratch_bytes(int C) {
+  return sizeof(float2) * static_cast<size_t>(C) * FftSmem<G>::SCR;
 }
 template <int G>
-static size_t fwd_cols_smem(const FftArgs& f) {
-  return sizeof(float2) * (G + 2 * static_cast<size_t>(f.N) * f.C + static_cast<size_t>(f.C) * FftSmem<G>::SCR) +
-         sizeof(uint32_t) * static_cast<size_t>(G) * (2 * f.C + 1);
+static size_t fwd_rows_region(const FftArgs& f) {
+  const size_t in = static_cast<size_t>(2 + f.C) * f.N * 8 + static_cast<size_t>(f.N) * 4;
+  const size_t out = sizeof(float2) * static_cast<size_t>(G) * (f.C + 1);
+  return align16(std::max({in, out, fft_scratch_bytes<G>(f.C)}));
 }
 template <int G>
-static size_t inv_cols_smem(const FftArgs& f) {
-  return sizeof(float2) * (G + 2 * static_cast<size_t>(G) * f.C + static_cast<size_t>(f.N) * (f.C + 1) +
-                           static_cast<size_t>(f.C) * FftSmem<G>::SCR);
+static size_t fwd_cols_region(const FftArgs& f) {
+  const size_t in = sizeof(float2) * static_cast<size_t>(f.N) * f.C;
+  const size_t out = sizeof(uint32_t) * static_cast<size_t>(G) * (2 * f.C + 1);
+  return align16(std::max({in, out, fft_scratch_bytes<G>(f.C)}));
 }
 template <int G>
-static size_t inv_rows_smem(const FftArgs& f) {
-  return inv_cols_smem<G>(f);
+static size_t inv_cols_region(const FftArgs& f) {
+  const size_t in = sizeof(float2) * static_cast<size_t>(G) * f.C;
+  const size_t out = sizeof(float2) * static_cast<size_t>(f.N) * (f.C + 1);
+  return align16(std::max({in, out, fft_scratch_bytes<G>(f.C)}));
+}
+template <int G>
+static size_t inv_rows_region(const FftArgs& f) {
+  const size_t in = sizeof(float2) * static_cast<size_t>(G) * f.C;
+  const size_t img = sizeof(float2) * static_cast<size_t>(f.C) * f.N;
+  return align16(std::max({in, img, fft_scratch_bytes<G>(f.C)}));
+}
+static size_t inv_rows_epi(const FftArgs& f, int mode) {
+  const size_t maps = f.smaps ? sizeof(float2) * static_cast<size_t>(f.C) * f.N : 0;
+  const size_t prow = mode == 2 ? sizeof(float2) * static_cast<size_t>(f.N) : 0;
+  return align16(maps + prow + sizeof(float) * static_cast<size_t>(f.N));
 }
 
 template <class K>
@@ -857,23 +892,41 @@ static int persistent_grid(K k, int threads, size_t smem, int items) {
     case 1024: { constexpr int GG = 1024; __VA_ARGS__; } break; \
     default: break;                                            \
   }
+// FFT stage instantiation by CTA size bound: up to 8 coils (three CTAs per SM) or 16
+#define TSN_FFT_MAXW(C_, ...)                   \
+  if ((C_) <= 8) {                              \
+    constexpr int MW = 8;                       \
+    __VA_ARGS__;                                \
+  } else {                                      \
+    constexpr int MW = 16;                      \
+    __VA_ARGS__;                                \
+  }
 
 void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
                      const double* partials, int nparts, CgState* st, int iter, cudaStream_t s) {
   TSN_G_SWITCH(f.G, {
-    const size_t sm = fwd_rows_smem<GG>(f);
-    ensure_smem(fwd_rows_kernel<GG>, sm);
-    const int grid = persistent_grid(fwd_rows_kernel<GG>, 32 * f.C, sm, f.N);
-    fwd_rows_kernel<GG><<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
+    const size_t sm = sizeof(float2) * GG + fwd_rows_region<GG>(f);
+    TSN_FFT_MAXW(f.C, {
+      auto k = fwd_rows_kernel<GG, MW>;
+      ensure_smem(k, sm);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.N);
+      k<<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
+    });
   });
 }
 
 void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStream_t s) {
   TSN_G_SWITCH(f.G, {
-    const size_t sm = fwd_cols_smem<GG>(f);
-    ensure_smem(fwd_cols_kernel<GG>, sm);
-    const int grid = persistent_grid(fwd_cols_kernel<GG>, 32 * f.C, sm, f.G);
-    fwd_cols_kernel<GG><<<grid, 32 * f.C, sm, s>>>(f, z1, panel);
+    const size_t region = fwd_cols_region<GG>(f);
+    const size_t base = sizeof(float2) * GG;
+    const int nbuf = base + 2 * region <= kFftTwoCtaSmem ? 2 : 1;
+    const size_t sm = base + nbuf * region;
+    TSN_FFT_MAXW(f.C, {
+      auto k = fwd_cols_kernel<GG, MW>;
+      ensure_smem(k, sm);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.G);
+      k<<<grid, 32 * f.C, sm, s>>>(f, z1, panel, static_cast<int>(region), nbuf);
+    });
   });
 }
 
@@ -886,21 +939,34 @@ void launch_split_samples(const float2* y, const float* density, int64_t m, int 
 
 void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStream_t s) {
   TSN_G_SWITCH(f.G, {
-    const size_t sm = inv_cols_smem<GG>(f);
-    ensure_smem(inv_cols_kernel<GG>, sm);
-    const int g = persistent_grid(inv_cols_kernel<GG>, 32 * f.C, sm, f.G);
-    inv_cols_kernel<GG><<<g, 32 * f.C, sm, s>>>(f, grid, w1);
+    const size_t region = inv_cols_region<GG>(f);
+    const size_t base = sizeof(float2) * GG;
+    const int nbuf = base + 2 * region <= kFftTwoCtaSmem ? 2 : 1;
+    const size_t sm = base + nbuf * region;
+    TSN_FFT_MAXW(f.C, {
+      auto k = inv_cols_kernel<GG, MW>;
+      ensure_smem(k, sm);
+      const int g = persistent_grid(k, 32 * f.C, sm, f.G);
+      k<<<g, 32 * f.C, sm, s>>>(f, grid, w1, static_cast<int>(region), nbuf);
+    });
   });
 }
 
 void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r, const float2* p,
                      double* partials, CgState* st, int iter, float inv_scale2, float lambda_scaled, cudaStream_t s) {
   TSN_G_SWITCH(f.G, {
-    const size_t sm = inv_rows_smem<GG>(f);
-    ensure_smem(inv_rows_kernel<GG>, sm);
-    const int g = persistent_grid(inv_rows_kernel<GG>, 32 * f.C, sm, f.N);
-    inv_rows_kernel<GG><<<g, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2,
-                                                 lambda_scaled);
+    const size_t region = inv_rows_region<GG>(f);
+    const size_t base = sizeof(float2) * GG + region;
+    const size_t epi = inv_rows_epi(f, mode);
+    const int epi_smem = base + epi <= kFftTwoCtaSmem ? 1 : 0;
+    const size_t sm = base + (epi_smem ? epi : 0);
+    TSN_FFT_MAXW(f.C, {
+      auto k = inv_rows_kernel<GG, MW>;
+      ensure_smem(k, sm);
+      const int g = persistent_grid(k, 32 * f.C, sm, f.N);
+      k<<<g, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2, lambda_scaled,
+                                static_cast<int>(region), epi_smem);
+    });
   });
 }
 

@@ -19,6 +19,8 @@
 //     tables.  Make that first call before any stream capture begins.
 //   * Every GPU that loads the library holds the arrays until the process exits.
 #include <cmath>
+#include <cstdint>
+#include <initializer_list>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -93,7 +95,10 @@ extern "C" tsn_status tsn_fft_adjoint_image_static(int32_t im_size, int32_t grid
     if (!grid_c64 || !scaling || !x) tsn::fail(TSN_ERR_ARG, "NULL argument");
     if (grid_size < 128 || grid_size > kMaxGrid || (grid_size & (grid_size - 1)))
       tsn::fail(TSN_ERR_UNSUPPORTED, "grid size must be a power of two in [128, 1024]");
-    if (im_size <= 0 || im_size % 2 || im_size > grid_size) tsn::fail(TSN_ERR_SHAPE, "need an even image size <= grid size");
+    if (im_size <= 0 || im_size % 4 || im_size > grid_size)
+      tsn::fail(TSN_ERR_SHAPE, "need an image size that is a multiple of 4 and <= grid size");
+    for (const void* p : {grid_c64, static_cast<const void*>(scaling), smaps, static_cast<const void*>(x)})
+      if (reinterpret_cast<uintptr_t>(p) & 15u) tsn::fail(TSN_ERR_ARG, "device arrays must be 16-byte aligned");
     if (coils < 4 || coils > 16 || coils % 4) tsn::fail(TSN_ERR_UNSUPPORTED, "coil count must be 4, 8, 12 or 16");
     const int64_t need = static_cast<int64_t>(grid_size) * im_size * coils;
     if (need > kStaticScratchElems)

@@ -5,7 +5,9 @@
 // nufft_fp16x2_cg_bench.cu:203-268 with one plan object and one CUDA graph per solve.
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -247,6 +249,15 @@ void need_fft(const tsn_plan* P) {
   const int G = P->G;
   if (G < 128 || G > 1024 || (G & (G - 1)))
     fail(TSN_ERR_UNSUPPORTED, "FFT endpoints need a power-of-two grid size in [128, 1024]");
+  // image rows (and FP32 deapodization rows) are streamed as whole 16-byte chunks
+  if (P->N % 4) fail(TSN_ERR_UNSUPPORTED, "FFT endpoints need an image size that is a multiple of 4");
+}
+
+// Device arrays the kernels stream with 16-byte copies (images, maps, samples, grids, panels)
+// must start on a 16-byte boundary; cudaMalloc and torch allocations always do.
+void need_aligned(std::initializer_list<const void*> ptrs) {
+  for (const void* p : ptrs)
+    if (p && (reinterpret_cast<uintptr_t>(p) & 15u)) fail(TSN_ERR_ARG, "device arrays must be 16-byte aligned");
 }
 
 void allocate_workspaces(tsn_plan* P) {
@@ -596,6 +607,7 @@ extern "C" {
 tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream) {
   try {
     if (!plan || !x || !y) fail(TSN_ERR_ARG, "NULL argument");
+    need_aligned({x, smaps, y});
     need_views(plan, true, false);
     enqueue_forward(plan, x, smaps, y, reinterpret_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
@@ -608,6 +620,7 @@ tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y
 tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream) {
   try {
     if (!plan || !x || !y) fail(TSN_ERR_ARG, "NULL argument");
+    need_aligned({x, smaps, y});
     need_views(plan, false, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     enqueue_adjoint_grid(plan, y, nullptr, s);
@@ -629,6 +642,8 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
     if (!plan || !y || !smaps || !x) fail(TSN_ERR_ARG, "NULL argument (y, smaps and x are required)");
     if (iters < 0 || iters > kMaxCgIter) fail(TSN_ERR_ARG, "iteration count out of range");
     if (!(operator_scale > 0.0f) || !std::isfinite(lambda)) fail(TSN_ERR_ARG, "invalid operator scale or lambda");
+    need_aligned({y, smaps, x});
+    if (reinterpret_cast<uintptr_t>(density) & 3u) fail(TSN_ERR_ARG, "density must be 4-byte aligned");
     need_views(plan, true, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     GraphKey key{y, smaps, density, x, iters, 0, 0, s};
@@ -688,6 +703,7 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
                               tsn_stream_t stream) {
   try {
     if (!plan || !y || !smaps || !stage_ms || reps <= 0) fail(TSN_ERR_ARG, "invalid argument");
+    need_aligned({y, smaps});
     need_views(plan, true, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     DeviceBuffer xbuf;
@@ -749,6 +765,7 @@ tsn_status tsn_fft_forward_panel(tsn_plan* plan, const void* x, const void* smap
                                  float* panel_scale, tsn_stream_t stream) {
   try {
     if (!plan || !x || !panel_f16) fail(TSN_ERR_ARG, "NULL argument");
+    need_aligned({x, smaps, panel_f16});
     need_views(plan, false, false);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const FftArgs f = fft_args(plan, smaps);
@@ -775,6 +792,7 @@ tsn_status tsn_fft_adjoint_image(tsn_plan* plan, const void* grid_c64, const voi
                                  tsn_stream_t stream) {
   try {
     if (!plan || !grid_c64 || !x) fail(TSN_ERR_ARG, "NULL argument");
+    need_aligned({grid_c64, smaps, x});
     need_views(plan, false, false);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const FftArgs f = fft_args(plan, smaps);
@@ -797,6 +815,7 @@ tsn_status tsn_interp_component(tsn_plan* plan, int32_t view, int32_t component,
                                 tsn_stream_t stream) {
   try {
     if (!plan || !dense_f16 || !out) fail(TSN_ERR_ARG, "NULL argument");
+    need_aligned({dense_f16, out});
     if (view != TSN_VIEW_G && view != TSN_VIEW_GT) fail(TSN_ERR_ARG, "unknown view");
     const DevView& d = plan->view[view];
     if (!d.present) fail(TSN_ERR_ARG, "plan lacks this view");
