@@ -90,7 +90,7 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.05)
+            time.sleep(0.002)
 
     def __enter__(self):
         if self._nv is not None:
@@ -210,31 +210,54 @@ def run_ours(args, cfg) -> dict:
     max_ms = float(t.item())
     value = world * args.steps / (max_ms / 1e3)
 
-    # end to end through the public call with host buffers: H2D of y and maps, D2H of x
+    # end to end through the public call with host buffers: every step copies its y and maps
+    # from pinned host memory and reads its image back.  The copy of step k+1 runs on a side
+    # stream while step k solves (double-buffered device inputs); the L2 flush between steps
+    # runs alone and its time is taken out of the total.
     y_h = y.cpu().pin_memory()
     s_h = smaps.cpu().pin_memory()
     x_h = torch.empty(x_out.shape, dtype=x_out.dtype).pin_memory()
-    y_d, s_d = torch.empty_like(y), torch.empty_like(smaps)
+    y_d = [torch.empty_like(y) for _ in range(2)]
+    s_d = [torch.empty_like(smaps) for _ in range(2)]
     e2e_steps = max(3, args.steps // 2)
+    main = torch.cuda.current_stream()
+    side = torch.cuda.Stream(device=dev)
 
-    def e2e_step():
-        y_d.copy_(y_h, non_blocking=True)
-        s_d.copy_(s_h, non_blocking=True)
-        plan.cg_sense(y_d, s_d, density=density, lam=lam, iters=iters, out=x_out, sync=False)
-        x_h.copy_(x_out, non_blocking=True)
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
 
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    es = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
-    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
-    for k in range(e2e_steps):
-        flush.zero_()
-        es[k].record()
-        e2e_step()
-        ee[k].record()
-    torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(es, ee))
+    def e2e_run(nsteps):
+        copied = [ev() for _ in range(nsteps + 1)]
+        f0 = [ev() for _ in range(nsteps)]
+        f1 = [ev() for _ in range(nsteps)]
+        start, end = ev(), ev()
+        start.record(main)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            y_d[0].copy_(y_h, non_blocking=True)
+            s_d[0].copy_(s_h, non_blocking=True)
+            copied[0].record(side)
+        for k in range(nsteps):
+            b = k & 1
+            main.wait_event(copied[k])     # inputs of step k are on the device; the next copy is done
+            f0[k].record(main)
+            flush.zero_()
+            f1[k].record(main)
+            if k + 1 < nsteps:             # next inputs stream in while this step solves
+                side.wait_event(f1[k])
+                with torch.cuda.stream(side):
+                    y_d[b ^ 1].copy_(y_h, non_blocking=True)
+                    s_d[b ^ 1].copy_(s_h, non_blocking=True)
+                    copied[k + 1].record(side)
+            plan.cg_sense(y_d[b], s_d[b], density=density, lam=lam, iters=iters, out=x_out, sync=False)
+            x_h.copy_(x_out, non_blocking=True)
+        end.record(main)
+        torch.cuda.synchronize()
+        flush_ms = sum(a.elapsed_time(b_) for a, b_ in zip(f0, f1))
+        return start.elapsed_time(end) - flush_ms
+
+    e2e_run(2)
+    e2e_ms = e2e_run(e2e_steps)
     te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
@@ -258,7 +281,8 @@ def run_ours(args, cfg) -> dict:
                    "tiles": plan.info["tiles"], "groups": plan.info["groups"]},
         "e2e": {"value": round(e2e_value, 3), "unit": "recons/s",
                 "h2d_bytes_per_step": int(y.numel() * 8 + smaps.numel() * 8),
-                "d2h_bytes_per_step": int(x_out.numel() * 8)},
+                "d2h_bytes_per_step": int(x_out.numel() * 8),
+                "overlap": "copy of step k+1 overlaps the solve of step k"},
         "gpu_launches": args.steps * (5 + 7 * iters + 1),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -326,7 +350,7 @@ def run_reference(args, cfg) -> dict | None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", choices=tuple(CONFIGS), default="headline")

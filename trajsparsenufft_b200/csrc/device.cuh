@@ -28,11 +28,18 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src));
 }
-// 16-byte copy that reads nothing and writes zeros when !valid (src-size 0); the source
-// must still be a mapped address.
-__device__ __forceinline__ void cp_async16_zfill(void* smem_dst, const void* gmem_src, bool valid) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src),
-               "r"(valid ? 16 : 0));
+// 16-byte copy when `live`, else a 16-byte zero store to the same shared address (no global
+// read); predicated, so a warp with mixed lanes does not branch.
+__device__ __forceinline__ void cp_async16_or_zero(void* smem_dst, const void* gmem_src, bool live) {
+  asm volatile(
+      "{\n"
+      "  .reg .pred p;\n"
+      "  setp.ne.b32 p, %2, 0;\n"
+      "  @p cp.async.cg.shared.global [%0], [%1], 16;\n"
+      "  @!p st.shared.v4.u32 [%0], {%3, %3, %3, %3};\n"
+      "}\n" ::"r"(smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(static_cast<int>(live)), "r"(0)
+      : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>

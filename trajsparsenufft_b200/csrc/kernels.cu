@@ -36,7 +36,8 @@ void set_twiddle_constants(cudaStream_t s) {
 // ------------------------------------------------------------------------------------------
 // Sparse interpolation: one warp per 16-row group, 2:4 tiles through mma.sp m16n8k32.
 // Per tile the 32 gathered panel rows (hi and res together) are brought to shared memory
-// with 16-byte cp.async (double-buffered), swizzled so ldmatrix.trans is conflict-free.
+// with 16-byte cp.async through a per-warp ring, swizzled so ldmatrix.trans is
+// conflict-free; dead (padding) columns are zero-stored and never read.
 // Reference: nufft_gt_spmma_complex_fused_f16_f32 (nufft_spmma_bench.cu:402-663), which
 // gathers B with 2-byte loads and reduces 4 warps through shared memory.
 // ------------------------------------------------------------------------------------------
@@ -50,14 +51,26 @@ __device__ __forceinline__ int chunk_swizzle(int ch, int row) {
 
 constexpr int kInterpWarps = 4;
 
+// Output row s (0..15) of a record: 24-bit little-endian fields, 0xFFFFFF = pad (-1).
+__device__ __forceinline__ int32_t record_row(const uint8_t* rows24, int s) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(rows24);
+  const int bit = 24 * s, off = bit & 31;
+  const uint32_t lo = w[bit >> 5];
+  const uint32_t hi = off > 8 ? w[(bit >> 5) + 1] : 0u;  // stays inside the 48-byte field
+  const uint32_t v = __funnelshift_r(lo, hi, off) & 0xFFFFFFu;
+  return v == static_cast<uint32_t>(kRecRowPad) ? -1 : static_cast<int32_t>(v);
+}
+
 // Per-warp shared-memory ring: stage = tile record (cols, A, meta) + 32 gathered panel rows.
 // Records are fetched kRecAhead tiles ahead, gathers kGatherAhead tiles ahead (the gather
 // needs the record's column ids), so a warp waits only on cp.async groups, never on a
 // register load.  Warps are persistent: each streams a contiguous, tile-balanced run of
-// work items and the pipeline runs across item boundaries.
-constexpr int kStages = 5;
-constexpr int kRecAhead = 4;
-constexpr int kGatherAhead = 2;
+// work items and the pipeline runs across item boundaries.  A four-stage ring (45 KB per
+// 4-warp CTA) keeps 20 warps per SM resident, which measured faster than deeper rings
+// with fewer warps.
+constexpr int kStages = 4;
+constexpr int kRecAhead = 3;
+constexpr int kGatherAhead = 1;
 
 // Writes one finished item: split chunks publish their accumulators and the last chunk of
 // the group reduces all chunks in chunk order; whole groups and finishing chunks apply the
@@ -165,7 +178,7 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   constexpr unsigned FULL = 0xFFFFFFFFu;
   static_assert(NACC <= kPartialFloats, "partials slot too small");
   static_assert(REC % 16 == 0 && STAGE % 16 == 0, "16-byte stages");
-  static_assert(kRecAhead == 4 && kGatherAhead == 2 && kStages == kRecAhead + 1, "group arithmetic");
+  static_assert(kGatherAhead >= 1 && kRecAhead > kGatherAhead && kStages == kRecAhead + 1, "ring arithmetic");
   extern __shared__ __align__(128) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wid = blockIdx.x * kInterpWarps + warp;
@@ -191,50 +204,46 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[c][a][i] = 0.f;
 
-  // k-th record of this warp -> its ring stage
-  auto issue_record = [&](int k) {
+  // Per-lane gather constants: chunk i of this lane is 16-byte chunk (lane + 32 i) % CH of
+  // gathered row (lane + 32 i) / CH; its swizzled shared offset and source byte offset.
+  int g_row[CH];
+  uint32_t g_dst[CH], g_src[CH];
+#pragma unroll
+  for (int i = 0; i < CH; ++i) {
+    const int ci = lane + 32 * i;
+    const int row = ci / CH, ch = ci % CH;
+    g_row[i] = row;
+    g_dst[i] = static_cast<uint32_t>(REC + row * BYTES + chunk_swizzle<CH>(ch, row) * 16);
+    g_src[i] = static_cast<uint32_t>(ch * 16);
+  }
+  // k-th record of this warp -> ring stage st
+  auto issue_record = [&](int k, uint8_t* st) {
     if (k < n) {
       const uint8_t* src = recs + static_cast<size_t>(k) * REC;
-      uint8_t* dst = ring + (k % kStages) * STAGE;
-      for (int c = lane; c < REC / 16; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
+#pragma unroll
+      for (int c0 = 0; c0 < REC / 16; c0 += 32)
+        if (c0 + 32 <= REC / 16 || lane < REC / 16 - c0) cp_async16(st + 16 * (c0 + lane), src + 16 * (c0 + lane));
     }
     cp_async_commit();  // empty groups keep the group arithmetic uniform
   };
-  auto issue_gather = [&](int k) {
+  auto issue_gather = [&](int k, uint8_t* st) {
     if (k >= 0 && k < n) {
-      uint8_t* st = ring + (k % kStages) * STAGE;
       const int32_t col = reinterpret_cast<const int32_t*>(st)[lane];
-      uint8_t* dst = st + REC;
 #pragma unroll
       for (int i = 0; i < CH; ++i) {
-        const int ci = lane + 32 * i;
-        const int row = ci / CH, ch = ci % CH;
-        const int src = __shfl_sync(FULL, col, row);
-        cp_async16_zfill(dst + row * BYTES + chunk_swizzle<CH>(ch, row) * 16,
-                         pb + static_cast<size_t>(max(src, 0)) * BYTES + ch * 16, src >= 0);
+        const int src = __shfl_sync(FULL, col, g_row[i]);
+        cp_async16_or_zero(st + g_dst[i], pb + static_cast<size_t>(static_cast<uint32_t>(max(src, 0)) * BYTES) + g_src[i],
+                           src >= 0);
       }
     }
     cp_async_commit();
   };
-  // Uniform iterations k = -kRecAhead .. n-1, two commit groups each (empty when out of
-  // range).  Newest-first the pending groups before the first "wait<4>" are
-  //   [rec(k+4), gat(k+1), rec(k+3), gat(k), rec(k+2), ...]   -> rec(k+2) has landed
-  // and after issuing gat(k+2)
-  //   [gat(k+2), rec(k+4), gat(k+1), rec(k+3), gat(k), ...]   -> gat(k) has landed.
-  for (int k = -kRecAhead; k < n; ++k) {
-    issue_record(k + kRecAhead);
-    cp_async_wait<4>();
-    __syncwarp();
-    issue_gather(k + kGatherAhead);
-    cp_async_wait<4>();
-    __syncwarp();
-    if (k < 0) continue;
-    uint8_t* st = ring + (k % kStages) * STAGE;
+  auto compute = [&](uint8_t* st) {
     const RecordInfo info = *reinterpret_cast<const RecordInfo*>(st + INFO);
-    const int32_t* trow = reinterpret_cast<const int32_t*>(st + INFO + 16);
+    const uint8_t* trow = st + INFO + 16;
     if constexpr (EPI == EPI_PANEL) {  // density weights at the item's first tile
       if (o.density && (info.flags & kRecFirst)) {
-        const int32_t r0 = trow[g], r1 = trow[g + 8];
+        const int32_t r0 = record_row(trow, g), r1 = record_row(trow, g + 8);
         wrow[0] = r0 >= 0 ? __ldg(o.density + r0) : 1.f;
         wrow[1] = r1 >= 0 ? __ldg(o.density + r1) : 1.f;
       }
@@ -259,10 +268,10 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
     }
     int32_t rows[2] = {-1, -1};
     if (info.flags & kRecLast) {
-      rows[0] = trow[g];
-      rows[1] = trow[g + 8];
+      rows[0] = record_row(trow, g);
+      rows[1] = record_row(trow, g + 8);
     }
-    __syncwarp();  // stage k is reused by record(k + kStages) next iteration
+    __syncwarp();  // this stage is refilled by the next iteration's record copy
     if (info.flags & kRecLast) {  // last tile of its item
       interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ>(acc, v, o, info, lane, rows, wrow, scale);
 #pragma unroll
@@ -271,6 +280,26 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
         for (int a2 = 0; a2 < NA; ++a2)
 #pragma unroll
           for (int i = 0; i < 4; ++i) acc[c][a2][i] = 0.f;
+    }
+  };
+  // Iterations k = -kRecAhead .. n-1, two commit groups each (empty when out of range):
+  // rec(k + R) then gat(k + Ga), with R = kRecAhead, Ga = kGatherAhead.  Tile k lives in
+  // stage (k + R) % kStages; unrolling by kStages makes every stage address a constant.
+  // After committing rec(k + R), the groups newer than rec(k + Ga) are gat(k + 2Ga - R)
+  // and the 2(R - Ga) - 1 groups of the later iterations, so wait<2(R - Ga)> lands the
+  // record the next gather reads; after committing gat(k + Ga), wait<2 Ga> lands gat(k).
+  for (int k0 = -kRecAhead; k0 < n; k0 += kStages) {
+#pragma unroll
+    for (int u = 0; u < kStages; ++u) {
+      const int k = k0 + u;
+      if (k >= n) break;
+      issue_record(k + kRecAhead, ring + ((u + kRecAhead) % kStages) * STAGE);
+      cp_async_wait<2 * (kRecAhead - kGatherAhead)>();
+      __syncwarp();
+      issue_gather(k + kGatherAhead, ring + ((u + kGatherAhead) % kStages) * STAGE);
+      cp_async_wait<2 * kGatherAhead>();
+      __syncwarp();
+      if (k >= 0) compute(ring + u * STAGE);
     }
   }
   cp_async_wait<0>();

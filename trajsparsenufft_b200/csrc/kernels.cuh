@@ -33,12 +33,17 @@ struct CgState {
 //   [128+576c, +512)         f16 compressed A of component c, [16][16]
 //   [640+576c, +64)          u32 mma.sp pair metadata of component c, [16]
 //   [128+576n, +16)          RecordInfo (n = component count)
-//   [128+576n+16, +64)       int32 output row of each of the 16 tile rows, -1 pad
+//   [128+576n+16, +48)       24-bit output row of each of the 16 tile rows (little endian,
+//                            0xFFFFFF = pad row)
+// A one-component record is 768 bytes: records and the gathered rows after them stay on
+// 128-byte boundaries.
 // Work item: a run of at most kChunkTiles tiles of one 16-row group. Groups with more
 // tiles are split; their chunks write raw accumulators to `partials` and the warp that
 // arrives last (counter) sums all chunks in chunk order, so results stay deterministic.
 constexpr int kChunkTiles = 8;
-constexpr int kRecInfoBytes = 80;
+constexpr int kRecInfoBytes = 64;
+constexpr int32_t kRecRowPad = 0xFFFFFF;
+constexpr int64_t kMaxInterpRows = kRecRowPad;  // output rows addressable by a record
 constexpr int kRecFirst = 1;  // first tile of a work item
 constexpr int kRecLast = 2;   // last tile of a work item: apply the epilogue
 struct RecordInfo {

@@ -139,6 +139,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   const int64_t tiles = h.tiles(), groups = h.groups();
   const int ncomp = static_cast<int>(h.a.size());
   const int rec = record_bytes(ncomp);
+  if (h.output_size >= kMaxInterpRows) fail(TSN_ERR_UNSUPPORTED, "too many output rows for 24-bit record rows");
   // work items: groups of at most kChunkTiles tiles run whole; longer groups are split into
   // chunks (scheduled first, they are the long poles) reduced in chunk order
   struct Item {
@@ -197,12 +198,12 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
       info.first_slot = it.first_slot;
       info.chunk = it.chunk | (it.nchunks << 16);
       std::memcpy(r + 128 + 576 * ncomp, &info, sizeof info);
-      int32_t orow[kMTile];
+      uint8_t* orow = r + 128 + 576 * ncomp + sizeof info;  // 24-bit little-endian rows
       for (int s = 0; s < kMTile; ++s) {
         const int32_t v = h.group_row_ids[static_cast<size_t>(it.group) * kMTile + s];
-        orow[s] = (v >= 0 && rows_are_cells) ? static_cast<int32_t>(cell_to_internal(v, P->G)) : v;
+        const int64_t row = v < 0 ? kRecRowPad : (rows_are_cells ? cell_to_internal(v, P->G) : v);
+        for (int k = 0; k < 3; ++k) orow[3 * s + k] = static_cast<uint8_t>((row >> (8 * k)) & 0xFF);
       }
-      std::memcpy(r + 128 + 576 * ncomp + sizeof info, orow, sizeof orow);
     }
     if (pos - run_start >= target) {
       ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(pos)));
