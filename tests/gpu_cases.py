@@ -24,6 +24,10 @@ def case(name: str):
         n, g, c, spokes, readout = 256, 512, 8, 256, 512
     elif name == "c16":
         n, g, c, spokes, readout = 128, 256, 16, 64, 256
+    elif name == "n192":          # grid 384 = 3 x 128: radix-3 FFT step
+        n, g, c, spokes, readout = 192, 384, 4, 24, 384
+    elif name == "n320":          # grid 640 = 5 x 128: radix-5 FFT step, 12 coils
+        n, g, c, spokes, readout = 320, 640, 12, 16, 640
     else:
         raise KeyError(name)
     traj = synth.golden_radial(spokes, readout)

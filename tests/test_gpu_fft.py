@@ -24,7 +24,8 @@ def _grid_from_image(img, g, shift):
 
 
 @pytest.mark.parametrize("name,layout", [("small", "centered"), ("small", "reference"), ("cfg0", "centered"),
-                                         ("headline", "centered"), ("c16", "reference")])
+                                         ("headline", "centered"), ("c16", "reference"), ("n192", "centered"),
+                                         ("n320", "reference")])
 def test_forward_panel_matches_numpy_fft(name, layout):
     from trajsparsenufft_b200.operator import Plan
     traj, x, s, n, g, c, j, _ = case(name)
@@ -42,7 +43,7 @@ def test_forward_panel_matches_numpy_fft(name, layout):
 
 
 @pytest.mark.parametrize("name,layout", [("small", "centered"), ("cfg0", "reference"), ("headline", "centered"),
-                                         ("c16", "centered")])
+                                         ("c16", "centered"), ("n192", "reference"), ("n320", "centered")])
 def test_adjoint_endpoint_matches_numpy_ifft(name, layout):
     from trajsparsenufft_b200.operator import Plan
     traj, x, s, n, g, c, j, _ = case(name)

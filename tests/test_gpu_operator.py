@@ -57,11 +57,12 @@ def test_raw_interpolation_matches_reference_bin(name, view):
         assert rel_l2(out, exact) <= 1e-6
 
 
-@pytest.mark.parametrize("layout", ["centered", "reference"])
-def test_forward_adjoint_match_oracle(layout):
-    traj, x, s, n, g, c, j, _ = case("small")
-    plan = _plan("small", reference_layout=(layout == "reference"))
-    xt, st, _ = torch_inputs("small")
+@pytest.mark.parametrize("name,layout", [("small", "centered"), ("small", "reference"), ("n192", "centered"),
+                                         ("n320", "reference")])
+def test_forward_adjoint_match_oracle(name, layout):
+    traj, x, s, n, g, c, j, _ = case(name)
+    plan = _plan(name, reference_layout=(layout == "reference"))
+    xt, st, _ = torch_inputs(name)
     y_gpu = plan.forward(xt, st).cpu().numpy()
     emu = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16", panel_mode="split2")
     ex = onudft.Nudft(traj, n)

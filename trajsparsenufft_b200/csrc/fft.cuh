@@ -1,4 +1,5 @@
-// Warp-level FFT of length G = 32*P (P in {4, 8, 16, 32}) in FP32 registers.
+// Warp-level FFT of length G = 32*P (P in {4, 8, 16, 32}, or R times such a length for
+// R in {3, 5}; see FftPlan) in FP32 registers.
 //
 // One warp transforms one G-point sequence held as P values per lane
 // (lane l, register j <-> element l + 32 j). Four-step decomposition G = P x 32:
@@ -99,16 +100,17 @@ struct WarpFftShape {
   static_assert(P * 32 == G && (P & (P - 1)) == 0 && P >= 4 && P <= 32, "G must be 32*P, P in {4..32}");
 };
 
-// tw: shared table exp(-2 pi i e / G), e in [0, G).
-template <int G, bool INV>
-__device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, const float2* tw) {
+// Power-of-two warp FFT. tw: shared table exp(-2 pi i e / (G * TS)), e in [0, G * TS); the
+// transform reads every TS-th entry (TS > 1 when it is the base of a mixed-radix length).
+template <int G, bool INV, int TS = 1>
+__device__ __forceinline__ void warp_fft_pow2(float2 (&v)[G / 32], float2* scratch, const float2* tw) {
   using S = WarpFftShape<G>;
   constexpr int P = S::P, T = S::T;
   const int lane = threadIdx.x & 31;
   dft_reg<P, INV>(v);
 #pragma unroll
   for (int k = 1; k < P; ++k) {
-    float2 w = tw[(lane * k) & (G - 1)];
+    float2 w = tw[TS * ((lane * k) & (G - 1))];
     if (INV) w.y = -w.y;
     v[k] = cmul(v[k], w);
   }
@@ -123,7 +125,7 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, c
   if (T > 1) {
 #pragma unroll
     for (int m = 1; m < P; ++m) {
-      float2 w = tw[(h * m * P) & (G - 1)];
+      float2 w = tw[TS * ((h * m * P) & (G - 1))];
       if (INV) w.y = -w.y;
       v[m] = cmul(v[m], w);
     }
@@ -166,7 +168,7 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, c
           float2 z;
           z.x = __shfl_sync(0xFFFFFFFFu, v[m].x, (lane & ~7) | h2);
           z.y = __shfl_sync(0xFFFFFFFFu, v[m].y, (lane & ~7) | h2);
-          float2 w = tw[((h2 * h) & 7) * (G / 8)];
+          float2 w = tw[TS * (((h2 * h) & 7) * (G / 8))];
           if (INV) w.y = -w.y;
           acc = cadd(acc, cmul(z, w));
         }
@@ -176,12 +178,86 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, c
   }
 }
 
-// Output element index held in register m after warp_fft.
+// Output element index held in register m after warp_fft_pow2<G>.
 template <int G>
-__device__ __forceinline__ int warp_fft_out_index(int m) {
+__device__ __forceinline__ int warp_fft_pow2_out_index(int m) {
   using S = WarpFftShape<G>;
   const int lane = threadIdx.x & 31;
   return lane / S::T + S::P * m + S::P * S::P * (lane % S::T);
+}
+
+// Lengths G = R * B with R in {1, 3, 5} and a power-of-two base B = 32 * 2^k >= 128; the
+// radix-3 and radix-5 factors give the grids 2N of image sizes N = 192 and 320.
+template <int G>
+struct FftPlan {
+  static constexpr int R = (G % 5 == 0) ? 5 : (G % 3 == 0) ? 3 : 1;
+  static constexpr int B = G / R;                           // power-of-two base length
+  static constexpr int P = G / 32;                          // registers per lane
+  static constexpr int PB = B / 32;                         // registers per lane of one base FFT
+  static constexpr int SCRATCH = WarpFftShape<B>::SCRATCH;  // float2 per warp
+};
+
+// Input element held in register j before warp_fft: lane + 32 j for power-of-two lengths;
+// for G = R B, register r * PB + j' holds x[R (lane + 32 j') + r] (decimation by R).
+template <int G>
+__device__ __forceinline__ int warp_fft_in_index(int j) {
+  using F = FftPlan<G>;
+  const int lane = threadIdx.x & 31;
+  if constexpr (F::R == 1) return lane + 32 * j;
+  else return F::R * (lane + 32 * (j % F::PB)) + j / F::PB;
+}
+
+// Output element index held in register m after warp_fft.
+template <int G>
+__device__ __forceinline__ int warp_fft_out_index(int m) {
+  using F = FftPlan<G>;
+  if constexpr (F::R == 1) return warp_fft_pow2_out_index<G>(m);
+  else return warp_fft_pow2_out_index<F::B>(m % F::PB) + F::B * (m / F::PB);
+}
+
+// Warp FFT of length G (see FftPlan). tw: shared table exp(-2 pi i e / G), e in [0, G).
+// For G = R B: R base FFTs of the decimated sequences Y_r, then for each base output k a
+// radix-R step in registers, X[k + B q] = sum_r W_G^{r k} Y_r[k] W_R^{r q}.
+template <int G, bool INV>
+__device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, const float2* tw) {
+  using F = FftPlan<G>;
+  if constexpr (F::R == 1) {
+    warp_fft_pow2<G, INV>(v, scratch, tw);
+  } else {
+    constexpr int R = F::R, B = F::B, PB = F::PB;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      float2 sub[PB];
+#pragma unroll
+      for (int j = 0; j < PB; ++j) sub[j] = v[r * PB + j];
+      warp_fft_pow2<B, INV, R>(sub, scratch, tw);  // W_B^e = tw[R e]
+#pragma unroll
+      for (int j = 0; j < PB; ++j) v[r * PB + j] = sub[j];
+    }
+#pragma unroll
+    for (int m = 0; m < PB; ++m) {
+      const int k = warp_fft_pow2_out_index<B>(m);
+      float2 t[R];
+      t[0] = v[m];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[r * k];  // r k < G
+        if (INV) w.y = -w.y;
+        t[r] = cmul(v[r * PB + m], w);
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        float2 acc = t[0];
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = tw[B * ((r * q) % R)];  // W_R^{r q} = W_G^{B (r q mod R)}
+          if (INV) w.y = -w.y;
+          acc = cadd(acc, cmul(t[r], w));
+        }
+        v[q * PB + m] = acc;
+      }
+    }
+  }
 }
 
 }  // namespace dev

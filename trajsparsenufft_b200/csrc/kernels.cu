@@ -399,7 +399,7 @@ __device__ __forceinline__ double sum_partials(const double* part, int nparts, d
 // ------------------------------------------------------------------------------------------
 template <int G>
 struct FftSmem {
-  static constexpr int SCR = WarpFftShape<G>::SCRATCH;
+  static constexpr int SCR = FftPlan<G>::SCRATCH;
 };
 
 // Copy `bytes` (multiple of 16) from global to shared with 16-byte cp.async, all threads.
@@ -428,11 +428,12 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
 }
 
 // The four FFT stages run one warp per coil in CTAs of 32*C threads (C <= MAXW). With
-// MAXW = 8 and G <= 512 the 80-register cap keeps three CTAs resident per SM. The per-warp
+// MAXW = 8 and G <= 512 the 80-register cap keeps three CTAs resident per SM (two at 128
+// registers for larger grids). The per-warp
 // FFT scratch and the output staging reuse the input slab's shared memory once it is
 // consumed, which keeps a CTA near 72 KB. The column stages double-buffer the slab when two
 // regions fit, so the next item streams in while the current one is transformed.
-#define TSN_FFT_BOUNDS(G, MAXW) __launch_bounds__((MAXW) * 32, ((MAXW) <= 8 && (G) <= 512) ? 3 : 1)
+#define TSN_FFT_BOUNDS(G, MAXW) __launch_bounds__((MAXW) * 32, (MAXW) > 8 ? 1 : ((G) <= 512 ? 3 : 2))
 
 // Forward rows (x-stage). Image row i0 -> z1[q1][i0][c] for all q1. Fuses the SENSE
 // multiply, deapodization, power-of-two panel scaling, zero-padding and (CG) p = r + beta p.
@@ -521,7 +522,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_rows_kernel(FftArgs f, const float2*
     const int c = warp;
 #pragma unroll
     for (int j = 0; j < P; ++j) {
-      const int n = lane + 32 * j;
+      const int n = warp_fft_in_index<G>(j);
       int i1 = n + f.shift;
       if (i1 >= G) i1 -= G;
       float2 val = make_float2(0.f, 0.f);
@@ -582,7 +583,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_cols_kernel(FftArgs f, const float2*
     float2 v[P];
 #pragma unroll
     for (int j = 0; j < P; ++j) {
-      const int n = lane + 32 * j;
+      const int n = warp_fft_in_index<G>(j);
       int i0 = n + f.shift;
       if (i0 >= G) i0 -= G;
       v[j] = i0 < N ? in_s[slab_idx(i0, c, C)] : make_float2(0.f, 0.f);
@@ -681,7 +682,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_cols_kernel(FftArgs f, const float2*
     const float2* in_s = reinterpret_cast<const float2*>(reg);
     float2 v[P];
 #pragma unroll
-    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
+    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(warp_fft_in_index<G>(j), c, C)];
     __syncthreads();
     warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
     __syncthreads();
@@ -757,7 +758,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2*
     const float2* in_s = reinterpret_cast<const float2*>(reg);
     float2 v[P];
 #pragma unroll
-    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(lane + 32 * j, c, C)];
+    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(warp_fft_in_index<G>(j), c, C)];
     __syncthreads();
     warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
     __syncthreads();
@@ -804,10 +805,26 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2*
   }
 }
 
+constexpr int kCgRowPix = 4;  // pixels per thread of cg_update: rows up to 1024 pixels at 256 threads
+
 __global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
                                  const float2* __restrict__ ap, const double* __restrict__ pap_parts,
                                  double* __restrict__ rr_parts, CgState* __restrict__ st, int iter) {
   __shared__ double red[33];
+  // the row's vectors stream in while the pAp partials are reduced (N <= kCgRowPix * blockDim)
+  const int i0 = blockIdx.x;
+  float2 pv[kCgRowPix], av[kCgRowPix], xv[kCgRowPix], rv[kCgRowPix];
+#pragma unroll
+  for (int j = 0; j < kCgRowPix; ++j) {
+    const int i1 = threadIdx.x + j * blockDim.x;
+    if (i1 < N) {
+      const size_t pix = static_cast<size_t>(i0) * N + i1;
+      pv[j] = p[pix];
+      av[j] = ap[pix];
+      xv[j] = x[pix];
+      rv[j] = r[pix];
+    }
+  }
   const double pap = sum_partials(pap_parts, N, red);
   const double rho = st->rho[iter];
   const bool ok = isfinite(pap) && pap > 0.0;
@@ -821,18 +838,18 @@ __global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restri
   }
   const float af = static_cast<float>(alpha);
   double acc = 0.0;
-  const int i0 = blockIdx.x;
-  for (int i1 = threadIdx.x; i1 < N; i1 += blockDim.x) {
+#pragma unroll
+  for (int j = 0; j < kCgRowPix; ++j) {
+    const int i1 = threadIdx.x + j * blockDim.x;
+    if (i1 >= N) continue;
     const size_t pix = static_cast<size_t>(i0) * N + i1;
-    const float2 pv = p[pix], av = ap[pix];
-    float2 xv = x[pix], rv = r[pix];
-    xv.x += af * pv.x;
-    xv.y += af * pv.y;
-    rv.x -= af * av.x;
-    rv.y -= af * av.y;
-    x[pix] = xv;
-    r[pix] = rv;
-    acc += static_cast<double>(rv.x) * rv.x + static_cast<double>(rv.y) * rv.y;
+    xv[j].x += af * pv[j].x;
+    xv[j].y += af * pv[j].y;
+    rv[j].x -= af * av[j].x;
+    rv[j].y -= af * av[j].y;
+    x[pix] = xv[j];
+    r[pix] = rv[j];
+    acc += static_cast<double>(rv[j].x) * rv[j].x + static_cast<double>(rv[j].y) * rv[j].y;
   }
   const double t = block_sum(acc, red);
   if (threadIdx.x == 0) rr_parts[i0] = t;
@@ -917,7 +934,9 @@ static int persistent_grid(K k, int threads, size_t smem, int items) {
   switch (G_) {                                                \
     case 128: { constexpr int GG = 128; __VA_ARGS__; } break;  \
     case 256: { constexpr int GG = 256; __VA_ARGS__; } break;  \
+    case 384: { constexpr int GG = 384; __VA_ARGS__; } break;  \
     case 512: { constexpr int GG = 512; __VA_ARGS__; } break;  \
+    case 640: { constexpr int GG = 640; __VA_ARGS__; } break;  \
     case 1024: { constexpr int GG = 1024; __VA_ARGS__; } break; \
     default: break;                                            \
   }

@@ -90,6 +90,11 @@ struct FftArgs {
 
 void set_twiddle_constants(cudaStream_t s);
 
+// Grid sizes the warp FFT stages are built for: 32 * 2^k (128..1024) and 3 * 128, 5 * 128.
+inline bool fft_grid_supported(int g) {
+  return g == 128 || g == 256 || g == 384 || g == 512 || g == 640 || g == 1024;
+}
+
 void launch_interp(const InterpView& v, const __half* panel, int rowh, bool split, int epi, bool conj,
                    const InterpOut& o, cudaStream_t s);
 // warps the persistent interpolation kernel keeps resident on this device for a panel row

@@ -93,8 +93,8 @@ extern "C" tsn_status tsn_fft_adjoint_image_static(int32_t im_size, int32_t grid
                                                    void* x, tsn_stream_t stream) {
   try {
     if (!grid_c64 || !scaling || !x) tsn::fail(TSN_ERR_ARG, "NULL argument");
-    if (grid_size < 128 || grid_size > kMaxGrid || (grid_size & (grid_size - 1)))
-      tsn::fail(TSN_ERR_UNSUPPORTED, "grid size must be a power of two in [128, 1024]");
+    if (!tsn::fft_grid_supported(grid_size) || grid_size > kMaxGrid)
+      tsn::fail(TSN_ERR_UNSUPPORTED, "grid size must be 128, 256, 384, 512, 640 or 1024");
     if (im_size <= 0 || im_size % 4 || im_size > grid_size)
       tsn::fail(TSN_ERR_SHAPE, "need an image size that is a multiple of 4 and <= grid size");
     for (const void* p : {grid_c64, static_cast<const void*>(scaling), smaps, static_cast<const void*>(x)})

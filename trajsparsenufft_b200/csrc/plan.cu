@@ -248,8 +248,8 @@ void check_desc(const tsn_plan_desc* d) {
 // FFT endpoints are built for power-of-two grids of 128..1024 points.
 void need_fft(const tsn_plan* P) {
   const int G = P->G;
-  if (G < 128 || G > 1024 || (G & (G - 1)))
-    fail(TSN_ERR_UNSUPPORTED, "FFT endpoints need a power-of-two grid size in [128, 1024]");
+  if (!fft_grid_supported(G))
+    fail(TSN_ERR_UNSUPPORTED, "FFT endpoints need a grid size of 128, 256, 384, 512, 640 or 1024");
   // image rows (and FP32 deapodization rows) are streamed as whole 16-byte chunks
   if (P->N % 4) fail(TSN_ERR_UNSUPPORTED, "FFT endpoints need an image size that is a multiple of 4");
 }
