@@ -9,6 +9,10 @@ phantoms / coil maps / trajectories (the reference measures on OCMR, which is no
 available); the measurement is the operator applied to the phantom plus 1e-3 rms noise.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config headline|cfg0|batch48]
+
+--config batch48 reconstructs a seeded uneven batch of 48 cases per step through the batched
+graph and reports the plain per-case drop-in (one solve after another) beside it.
 
 Multi-GPU (torchrun, one process per GPU) runs independent replicas: every rank
 reconstructs its own frames with no collective on the data path; value = all ranks'
@@ -37,6 +41,7 @@ METRIC = "CG-SENSE recons/s 256²x8coil x10CG at NRMSE<=0.2% vs FP64: batched/gr
 CONFIGS = {
     "headline": dict(n=256, g=512, c=8, spokes=256, readout=512, width=6, iters=10, density=False),
     "cfg0": dict(n=128, g=256, c=4, spokes=96, readout=256, width=6, iters=10, density=True),
+    "batch48": dict(batch=True, cases=48, streams=8, width=6, iters=10),
 }
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
@@ -316,20 +321,191 @@ def cpu_baseline(cfg, traj, x_np, s_np, y_np, sample_iters: int) -> dict:
             "seconds_per_recon": round(t_recon, 3)}
 
 
+def run_batch(args, cfg) -> dict | None:
+    """Uneven 48-case batch: the batched graph (tsn_batch_cg_sense) against the plain per-case
+    drop-in (one tsn_cg_sense graph per case, back to back on one stream), same inputs."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from trajsparsenufft_b200 import synth
+    from trajsparsenufft_b200.operator import Batch, Plan
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    specs = synth.uneven_batch(cfg["cases"], 20260823 + 1000 * rank)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=4) as ex:  # ctypes releases the GIL; the planner threads inside
+        plans = list(ex.map(lambda sp: Plan.from_trajectory(sp["trajectory"], im_size=sp["n"], grid_size=sp["g"],
+                                                            coils=sp["c"], width=cfg["width"], device=local), specs))
+    plan_s = time.perf_counter() - t0
+    ys, maps = [], []
+    for sp, pl in zip(specs, plans):
+        x = torch.from_numpy(synth.ellipse_phantom(sp["n"], sp["seed"])).to(dev)
+        s = torch.from_numpy(synth.coil_maps(sp["n"], sp["c"], sp["seed"])).to(dev)
+        yc = pl.forward(x, s)
+        g = torch.Generator(device=dev).manual_seed(sp["seed"])
+        rms = yc.abs().pow(2).mean().sqrt()
+        noise = torch.complex(torch.randn(yc.shape, device=dev, generator=g),
+                              torch.randn(yc.shape, device=dev, generator=g))
+        ys.append((yc + noise * (1e-3 * rms / math.sqrt(2.0))).contiguous())
+        maps.append(s)
+    outs = [torch.empty((sp["n"], sp["n"]), dtype=torch.complex64, device=dev) for sp in specs]
+    iters, lam = cfg["iters"], 1e-4
+    batch = Batch(plans, streams=cfg["streams"])
+    _, statuses = batch.cg_sense(ys, maps, lam=lam, iters=iters, outs=outs, sync=True)
+    bad = [i for i, st in enumerate(statuses) if "failure" in st]
+    if bad:
+        raise RuntimeError(f"CG status failure in cases {bad}")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def plain_step():
+        for pl, y, s, o in zip(plans, ys, maps, outs):
+            pl.cg_sense(y, s, lam=lam, iters=iters, out=o, sync=False)
+
+    def batch_step():
+        batch.cg_sense(ys, maps, lam=lam, iters=iters, outs=outs, sync=False)
+
+    def timed(step):
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+        torch.cuda.synchronize()
+        st = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        en = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            st[k].record()
+            step()
+            en[k].record()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in zip(st, en))
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    plain_ms = timed(plain_step)
+    with ClockSampler(local) as clocks:
+        batch_ms = timed(batch_step)
+    n_cases = len(specs)
+    value = world * n_cases * args.steps / (batch_ms / 1e3)
+    plain_value = world * n_cases * args.steps / (plain_ms / 1e3)
+
+    # end to end: every step copies all cases' y and maps from pinned host memory (side stream,
+    # overlapping the previous step's solve) and reads every image back
+    y_h = [y.cpu().pin_memory() for y in ys]
+    s_h = [s.cpu().pin_memory() for s in maps]
+    x_h = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
+    y_d = [[torch.empty_like(y) for y in ys] for _ in range(2)]
+    s_d = [[torch.empty_like(s) for s in maps] for _ in range(2)]
+    main = torch.cuda.current_stream()
+    side = torch.cuda.Stream(device=dev)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def copy_in(b):
+        for a, h in zip(y_d[b], y_h):
+            a.copy_(h, non_blocking=True)
+        for a, h in zip(s_d[b], s_h):
+            a.copy_(h, non_blocking=True)
+
+    def e2e_run(nsteps):
+        copied = [ev() for _ in range(nsteps + 1)]
+        f0 = [ev() for _ in range(nsteps)]
+        f1 = [ev() for _ in range(nsteps)]
+        start, end = ev(), ev()
+        start.record(main)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            copy_in(0)
+            copied[0].record(side)
+        for k in range(nsteps):
+            b = k & 1
+            main.wait_event(copied[k])
+            f0[k].record(main)
+            flush.zero_()
+            f1[k].record(main)
+            if k + 1 < nsteps:
+                side.wait_event(f1[k])
+                with torch.cuda.stream(side):
+                    copy_in(b ^ 1)
+                    copied[k + 1].record(side)
+            batch.cg_sense(y_d[b], s_d[b], lam=lam, iters=iters, outs=outs, sync=False)
+            for h, o in zip(x_h, outs):
+                h.copy_(o, non_blocking=True)
+        end.record(main)
+        torch.cuda.synchronize()
+        return start.elapsed_time(end) - sum(a.elapsed_time(b_) for a, b_ in zip(f0, f1))
+
+    e2e_steps = max(3, args.steps // 2)
+    e2e_run(2)
+    e2e_ms = e2e_run(e2e_steps)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.destroy_process_group()
+    e2e_value = world * n_cases * e2e_steps / (float(te.item()) / 1e3)
+    samples = sum(len(sp["trajectory"]) * sp["c"] for sp in specs)
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "recons/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(batch_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16x2->f32 (f64 CG scalars)", "data": "synthetic",
+        "config": {"workload": f"uneven batch of {n_cases} cases per step (synth.uneven_batch): N in "
+                               "{128,192,256,320} (grid 2N), coils in {4,8,12,16}, half golden-angle radial "
+                               "(64-384 spokes x 2N), half variable-density spirals (8-32 x 2048-4096), KB J=6, "
+                               f"{iters} CG iterations",
+                   "cases": n_cases, "streams": cfg["streams"], "recons_per_step": n_cases,
+                   "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
+                   "plan_seconds": round(plan_s, 1)},
+        "plain_per_case": {"value": round(plain_value, 3), "unit": "recons/s",
+                           "ms_per_step": round(plain_ms / args.steps, 4)},
+        "batch_speedup": round(value / plain_value, 3),
+        "nonuniform_samples_per_s": round(value / n_cases * samples * iters * 2, 1),
+        "e2e": {"value": round(e2e_value, 3), "unit": "recons/s",
+                "h2d_bytes_per_step": int(sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)),
+                "d2h_bytes_per_step": int(sum(o.numel() * 8 for o in outs)),
+                "overlap": "copies of step k+1 overlap the solve of step k"},
+        "gpu_launches": args.steps * n_cases * (5 + 7 * iters + 1),
+        "clocks": clocks.summary(),
+    }
+    return out if rank == 0 else None
+
+
 def run_reference(args, cfg) -> dict | None:
     """Reference arm: the reference's CPU FP32 CG-SENSE path (restated port) on host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
     from oracle.cpu_ref import CpuSenseFp32
-    from oracle.operator import KbSenseOperator
-    traj, x_np, s_np, _ = synth_inputs(cfg, 20260823)
     threads = os.cpu_count() or 1
-    op = CpuSenseFp32(traj, cfg["n"], cfg["g"], cfg["width"], s_np, threads=threads)
-    y = op.forward(x_np)
-    times = []
     sample_iters = 1
+    if cfg.get("batch"):  # a bounded sample: the first cases of the batch, one per step in turn
+        from trajsparsenufft_b200 import synth
+        specs = synth.uneven_batch(cfg["cases"], 20260823)[:4]
+        cases = [(sp["trajectory"], synth.ellipse_phantom(sp["n"], sp["seed"]),
+                  synth.coil_maps(sp["n"], sp["c"], sp["seed"]), sp["n"], sp["g"]) for sp in specs]
+        workload = f"cases 0-3 of the {cfg['cases']}-case uneven batch (synth.uneven_batch)"
+    else:
+        traj, x_np, s_np, _ = synth_inputs(cfg, 20260823)
+        cases = [(traj, x_np, s_np, cfg["n"], cfg["g"])]
+        workload = workload_text(cfg)
+    ops = []
+    for traj, x_np, s_np, n, g in cases:
+        op = CpuSenseFp32(traj, n, g, cfg["width"], s_np, threads=threads)
+        ops.append((op, op.forward(x_np)))
+    times = []
     for k in range(args.warmup + args.steps):
+        op, y = ops[k % len(ops)]
         _, _, t_rhs, t_iter = op.cg_sense(y, cfg["iters"], 1e-4, sample_iterations=sample_iters)
         if k >= args.warmup:
             times.append(t_rhs + cfg["iters"] * t_iter)
@@ -339,10 +515,10 @@ def run_reference(args, cfg) -> dict | None:
         "metric": METRIC, "impl": "reference", "value": round(value, 5), "unit": "recons/s", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_text(cfg)},
+        "config": {"workload": workload},
         "cpu_baseline": {"value": round(value, 5), "unit": "recons/s", "cores": threads, "kind": "port",
-                         "sample": f"per step: adjoint RHS + {sample_iters} of {cfg['iters']} FP32 CG iterations, "
-                                   "extrapolated to one reconstruction"},
+                         "sample": f"per step: adjoint RHS + {sample_iters} of {cfg['iters']} FP32 CG iterations of "
+                                   f"one case ({workload}), extrapolated to one reconstruction"},
         "e2e": {"value": round(value, 5), "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -359,7 +535,12 @@ def main() -> int:
     if args.warmup < 3:
         args.warmup = 3
     cfg = CONFIGS[args.config]
-    out = run_reference(args, cfg) if args.impl == "reference" else run_ours(args, cfg)
+    if args.impl == "reference":
+        out = run_reference(args, cfg)
+    elif cfg.get("batch"):
+        out = run_batch(args, cfg)
+    else:
+        out = run_ours(args, cfg)
     if out is not None:
         print(json.dumps(out), flush=True)
     return 0

@@ -190,6 +190,26 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
                         float lambda, float operator_scale, int32_t iters, void* x,
                         double* residual_history, tsn_cg_status* status, tsn_stream_t stream);
 
+/* ---- batches of independent reconstructions ------------------------------------------- */
+/* The reference runs one case per CG process (nufft_fp16x2_cg_bench.cu:279-297 argv).  A
+ * batch holds `count` plans of one device (any image size, coil count and trajectory) and
+ * solves them together: one CUDA graph forks the cases over `streams` streams (0: up to 8)
+ * and every persistent launch of a case uses a 1/streams slice of the GPU, so small cases run
+ * side by side instead of one after another.  Cases go to streams longest-first by estimated
+ * cost.  The plans stay owned by the caller and must outlive the batch; a plan may belong to
+ * one batch and must not run elsewhere while a batch solve is in flight. */
+typedef struct tsn_batch tsn_batch;
+tsn_status tsn_batch_create(tsn_plan* const* plans, int32_t count, int32_t streams, tsn_batch** out);
+tsn_status tsn_batch_destroy(tsn_batch* batch);
+/* CG-SENSE of every case (arrays of `count` device pointers; density may be NULL or hold NULL
+ * entries) with one lambda, operator scale and iteration count.  statuses (host, `count`
+ * entries) may be NULL; when given, the call synchronizes and returns the first failing
+ * case's status (NONFINITE / CURVATURE) after filling every entry. */
+tsn_status tsn_batch_cg_sense(tsn_batch* batch, const void* const* y, const void* const* smaps,
+                              const float* const* density, float lambda, float operator_scale,
+                              int32_t iters, void* const* x, tsn_cg_status* statuses,
+                              tsn_stream_t stream);
+
 /* ---- FFT endpoints (the role of nufft_custom_fft_f30_api.h:6-34) ---------------------- */
 /* Forward endpoint: panel[G*G][4C] f16 = s * FFT_G(pad(x * S_c * scaling)), rows q1*G + q0
  * (q1-major), each row = FP16 high parts then FP16 residuals, (re, im) interleaved per coil;

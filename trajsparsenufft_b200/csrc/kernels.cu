@@ -921,12 +921,13 @@ static int sm_count() {
   return n;
 }
 
-// persistent grid: resident CTAs per SM x SMs, capped by the item count
+// persistent grid: resident CTAs per SM x SMs (a 1/share slice of them when batched cases
+// run side by side), capped by the item count
 template <class K>
-static int persistent_grid(K k, int threads, size_t smem, int items) {
+static int persistent_grid(K k, int threads, size_t smem, int items, int share = 1) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
-  const int grid = std::max(1, per_sm) * sm_count();
+  const int grid = std::max(1, std::max(1, per_sm) * sm_count() / std::max(1, share));
   return std::max(1, std::min(grid, items));
 }
 
@@ -957,7 +958,7 @@ void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, fl
     TSN_FFT_MAXW(f.C, {
       auto k = fwd_rows_kernel<GG, MW>;
       ensure_smem(k, sm);
-      const int grid = persistent_grid(k, 32 * f.C, sm, f.N);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.N, f.share);
       k<<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
     });
   });
@@ -972,7 +973,7 @@ void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStre
     TSN_FFT_MAXW(f.C, {
       auto k = fwd_cols_kernel<GG, MW>;
       ensure_smem(k, sm);
-      const int grid = persistent_grid(k, 32 * f.C, sm, f.G);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.G, f.share);
       k<<<grid, 32 * f.C, sm, s>>>(f, z1, panel, static_cast<int>(region), nbuf);
     });
   });
@@ -994,7 +995,7 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
     TSN_FFT_MAXW(f.C, {
       auto k = inv_cols_kernel<GG, MW>;
       ensure_smem(k, sm);
-      const int g = persistent_grid(k, 32 * f.C, sm, f.G);
+      const int g = persistent_grid(k, 32 * f.C, sm, f.G, f.share);
       k<<<g, 32 * f.C, sm, s>>>(f, grid, w1, static_cast<int>(region), nbuf);
     });
   });
@@ -1011,7 +1012,7 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
     TSN_FFT_MAXW(f.C, {
       auto k = inv_rows_kernel<GG, MW>;
       ensure_smem(k, sm);
-      const int g = persistent_grid(k, 32 * f.C, sm, f.N);
+      const int g = persistent_grid(k, 32 * f.C, sm, f.N, f.share);
       k<<<g, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2, lambda_scaled,
                                 static_cast<int>(region), epi_smem);
     });

@@ -86,6 +86,7 @@ struct FftArgs {
   const float2* tw = nullptr;           // exp(-2 pi i e/G), e in [0,G)
   const float* scaling = nullptr;       // [N][N] deapodization
   const float2* smaps = nullptr;        // [C][N][N] or null
+  int share = 1;                        // persistent grids use 1/share of the resident CTAs
 };
 
 void set_twiddle_constants(cudaStream_t s);

@@ -3,6 +3,7 @@
 // tsn_interp_component. Replaces load_direction + launch_integrated_once + launch_cg of
 // experiments/production/src/nufft_integrated_bench.cu:135-226, :604-674 and
 // nufft_fp16x2_cg_bench.cu:203-268 with one plan object and one CUDA graph per solve.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -73,6 +74,11 @@ struct HostView {
 struct DevView {
   DeviceBuffer records, counters, partials, ranges;
   InterpView v;
+  // warp runs cut for a 1/share slice of the GPU (batched cases run side by side)
+  std::vector<int64_t> item_ends;  // record position after each work item, stream order
+  DeviceBuffer ranges_shared;
+  InterpView v_shared;
+  int share = 0;
   int64_t tiles = 0, groups = 0, active_rows = 0, nnz = 0, output_size = 0, n_cols = 0;
   bool present = false;
 };
@@ -105,6 +111,23 @@ struct tsn_plan {
   }
 };
 
+struct tsn_batch {
+  std::vector<tsn_plan*> plans;
+  std::vector<int> lane;             // stream of each case
+  int streams = 1;
+  int device = 0;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs;
+  ~tsn_batch() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (cudaEvent_t e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    for (cudaStream_t st : side) cudaStreamDestroy(st);
+  }
+};
+
 namespace {
 
 // reference cell index q0*G + q1 -> internal q1*G + q0
@@ -132,6 +155,20 @@ uint32_t live_columns(const HostView& h, int64_t t) {
     }
   }
   return m;
+}
+
+// Persistent-warp runs: contiguous item runs of about tiles / warps tiles each.
+std::vector<int2> cut_ranges(const std::vector<int64_t>& item_ends, int64_t tiles, int warps) {
+  const int64_t target = std::max<int64_t>(1, (tiles + warps - 1) / std::max(1, warps));
+  std::vector<int2> ranges;
+  int64_t run_start = 0;
+  for (int64_t e : item_ends)
+    if (e - run_start >= target) {
+      ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(e)));
+      run_start = e;
+    }
+  if (run_start < tiles) ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(tiles)));
+  return ranges;
 }
 
 void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
@@ -167,11 +204,9 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   items.insert(items.end(), small.begin(), small.end());
   // persistent warps: contiguous runs of items with about the same number of tiles each;
   // records are stored in that stream order so each warp reads one contiguous range
-  const int resident = interp_resident_warps(4 * P->C, ncomp);
-  const int64_t target = std::max<int64_t>(1, (tiles + resident - 1) / resident);
-  std::vector<int2> ranges;
   std::vector<uint8_t> records(static_cast<size_t>(tiles) * rec, 0);
-  int64_t pos = 0, run_start = 0;
+  d.item_ends.clear();
+  int64_t pos = 0;
   for (const Item& it : items) {
     for (uint32_t t = it.t0; t < it.t1; ++t, ++pos) {
       uint8_t* r = records.data() + pos * rec;
@@ -205,13 +240,10 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
         for (int k = 0; k < 3; ++k) orow[3 * s + k] = static_cast<uint8_t>((row >> (8 * k)) & 0xFF);
       }
     }
-    if (pos - run_start >= target) {
-      ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(pos)));
-      run_start = pos;
-    }
+    d.item_ends.push_back(pos);
   }
   if (pos != tiles) fail(TSN_ERR_FORMAT, "group offsets do not cover the tiles");
-  if (run_start < pos) ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(pos)));
+  const std::vector<int2> ranges = cut_ranges(d.item_ends, tiles, interp_resident_warps(4 * P->C, ncomp));
   d.records.upload(records);
   d.counters.upload(std::vector<int32_t>(std::max(nsplit, 1), 0));
   d.partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kPartialFloats * 32);
@@ -231,6 +263,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   d.output_size = h.output_size;
   d.n_cols = h.n_cols;
   d.present = true;
+  d.share = 0;
   P->info.groups[which] = groups;
   P->info.tiles[which] = tiles;
   P->info.active_rows[which] = h.active_rows;
@@ -289,8 +322,9 @@ void allocate_workspaces(tsn_plan* P) {
   CUDA_OK(cudaGetLastError());
 }
 
-FftArgs fft_args(const tsn_plan* P, const void* smaps) {
+FftArgs fft_args(const tsn_plan* P, const void* smaps, int share = 1) {
   FftArgs f;
+  f.share = share;
   f.N = P->N;
   f.G = P->G;
   f.C = P->C;
@@ -556,7 +590,28 @@ void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cud
   launch_interp(P->view[TSN_VIEW_G].v, P->panel.as<__half>(), P->rowh, true, EPI_SAMPLES, false, o, s);
 }
 
-void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cudaStream_t s) {
+// Cuts (once per share value, outside any stream capture) the interpolation warp runs for a
+// 1/share slice of the GPU, so cases of a batch run their launches side by side.
+void prepare_share(tsn_plan* P, int share) {
+  if (share <= 1) return;
+  for (DevView& d : P->view) {
+    if (!d.present || d.share == share) continue;
+    const int warps = std::max(kInterpWarpsPerCta, interp_resident_warps(4 * P->C, d.v.ncomp) / share);
+    const std::vector<int2> ranges = cut_ranges(d.item_ends, d.tiles, warps);
+    d.ranges_shared.upload(ranges);
+    d.v_shared = d.v;
+    d.v_shared.warp_ranges = d.ranges_shared.as<int2>();
+    d.v_shared.n_warps = static_cast<int32_t>(ranges.size());
+    d.share = share;
+  }
+}
+
+const InterpView& interp_view(const tsn_plan* P, int which, int share) {
+  const DevView& d = P->view[which];
+  return share > 1 ? d.v_shared : d.v;
+}
+
+void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cudaStream_t s, int share = 1) {
   CgState* st = P->state.as<CgState>();
   launch_norm_partials(static_cast<const float2*>(y), P->M * P->C, P->norm_parts.as<double>(), s);
   launch_split_samples(static_cast<const float2*>(y), density, P->M, P->C, P->spanel.as<__half>(),
@@ -565,19 +620,19 @@ void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cuda
   o.c64 = P->grid.as<float2>();
   o.rows = static_cast<int64_t>(P->G) * P->G;
   o.coils = P->C;
-  launch_interp(P->view[TSN_VIEW_GT].v, P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, o, s);
+  launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, o, s);
 }
 
 void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* density, float lambda, float scale,
-                int iters, void* x, cudaStream_t s) {
-  const FftArgs f = fft_args(P, smaps);
+                int iters, void* x, cudaStream_t s, int share = 1) {
+  const FftArgs f = fft_args(P, smaps, share);
   CgState* st = P->state.as<CgState>();
   const float inv_s2 = 1.0f / (scale * scale);
   const float lam = lambda * inv_s2;
   float2* X = static_cast<float2*>(x);
   float2 *R = P->r.as<float2>(), *Pv = P->p.as<float2>(), *AP = P->ap.as<float2>();
   double *pap = P->parts_pap.as<double>(), *rr = P->parts_rr.as<double>();
-  enqueue_adjoint_grid(P, y, density, s);
+  enqueue_adjoint_grid(P, y, density, s, share);
   launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
   launch_inv_rows(f, P->z1.as<float2>(), nullptr, 1, X, R, nullptr, rr, st, 0, inv_s2, 0.f, s);
   for (int k = 0; k < iters; ++k) {
@@ -588,17 +643,45 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     of.density = density;
     of.rows = P->M;
     of.coils = P->C;
-    launch_interp(P->view[TSN_VIEW_G].v, P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
+    launch_interp(interp_view(P, TSN_VIEW_G, share), P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
     InterpOut oa;
     oa.c64 = P->grid.as<float2>();
     oa.rows = static_cast<int64_t>(P->G) * P->G;
     oa.coils = P->C;
-    launch_interp(P->view[TSN_VIEW_GT].v, P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
+    launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
     launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
     launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, k, inv_s2, lam, s);
     launch_cg_update(P->N, X, R, Pv, AP, pap, rr, st, k, s);
   }
   launch_cg_finish(P->N, rr, st, iters, s);
+}
+
+// Reads a finished solve's scalar state (synchronizes s) into the optional host outputs and
+// returns the failure status of the solve (TSN_OK when finite with positive curvature).
+tsn_status read_cg_state(const tsn_plan* P, int iters, double* residual_history, tsn_cg_status* status,
+                         cudaStream_t s) {
+  CgState host;
+  CUDA_OK(cudaMemcpyAsync(&host, P->state.ptr, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+  CUDA_OK(cudaStreamSynchronize(s));
+  if (residual_history)
+    for (int k = 0; k <= iters; ++k) residual_history[k] = std::sqrt(std::max(host.rho[k], 0.0));
+  if (status) {
+    status->completed_iterations = host.completed;
+    status->positive_curvature = host.curvature_ok;
+    status->finite = host.finite_ok && std::isfinite(host.rho[iters]);
+    status->timeout = 0;
+    status->residual0 = std::sqrt(std::max(host.rho[0], 0.0));
+    status->residual_final = std::sqrt(std::max(host.rho[iters], 0.0));
+  }
+  if (!host.finite_ok || !std::isfinite(host.rho[iters])) return TSN_ERR_NONFINITE;
+  if (!host.curvature_ok) return TSN_ERR_CURVATURE;
+  return TSN_OK;
+}
+
+// Rough cost of one CG iteration of a plan in tile units (sparse tiles plus FFT points).
+double case_cost(const tsn_plan* P) {
+  return static_cast<double>(P->view[TSN_VIEW_G].tiles + P->view[TSN_VIEW_GT].tiles) +
+         static_cast<double>(P->C) * P->G * P->G / 25.0;
 }
 
 }  // namespace
@@ -678,21 +761,142 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
     }
     CUDA_OK(cudaGraphLaunch(it->second, s));
     if (residual_history || status) {
-      CgState host;
-      CUDA_OK(cudaMemcpyAsync(&host, plan->state.ptr, sizeof(CgState), cudaMemcpyDeviceToHost, s));
-      CUDA_OK(cudaStreamSynchronize(s));
-      if (residual_history)
-        for (int k = 0; k <= iters; ++k) residual_history[k] = std::sqrt(std::max(host.rho[k], 0.0));
-      if (status) {
-        status->completed_iterations = host.completed;
-        status->positive_curvature = host.curvature_ok;
-        status->finite = host.finite_ok && std::isfinite(host.rho[iters]);
-        status->timeout = 0;
-        status->residual0 = std::sqrt(std::max(host.rho[0], 0.0));
-        status->residual_final = std::sqrt(std::max(host.rho[iters], 0.0));
+      const tsn_status rc = read_cg_state(plan, iters, residual_history, status, s);
+      if (rc == TSN_ERR_NONFINITE) fail(TSN_ERR_NONFINITE, "CG produced non-finite values");
+      if (rc == TSN_ERR_CURVATURE) fail(TSN_ERR_CURVATURE, "CG denominator <= 0 (positive_curvature = 0)");
+    }
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_batch_create(tsn_plan* const* plans, int32_t count, int32_t streams, tsn_batch** out) {
+  try {
+    if (!plans || !out || count <= 0) fail(TSN_ERR_ARG, "invalid argument");
+    *out = nullptr;
+    auto b = std::make_unique<tsn_batch>();
+    b->plans.assign(plans, plans + count);
+    for (tsn_plan* P : b->plans) {
+      if (!P) fail(TSN_ERR_ARG, "NULL plan in batch");
+      need_views(P, true, true);
+      if (P->desc.device != b->plans[0]->desc.device) fail(TSN_ERR_ARG, "batch plans must share one device");
+    }
+    b->device = b->plans[0]->desc.device;
+    CUDA_OK(cudaSetDevice(b->device));
+    b->streams = std::max(1, std::min<int>(count, streams > 0 ? streams : 8));
+    // longest-first onto the least-loaded stream
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return case_cost(b->plans[a]) > case_cost(b->plans[c]); });
+    std::vector<double> load(b->streams, 0.0);
+    b->lane.assign(count, 0);
+    for (int i : order) {
+      const int k = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      b->lane[i] = k;
+      load[k] += case_cost(b->plans[i]);
+    }
+    for (tsn_plan* P : b->plans) prepare_share(P, b->streams);
+    b->side.resize(b->streams);
+    b->join.resize(b->streams);
+    CUDA_OK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (int k = 0; k < b->streams; ++k) {
+      CUDA_OK(cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking));
+      CUDA_OK(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+    }
+    CUDA_OK(cudaGetLastError());
+    *out = b.release();
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_batch_destroy(tsn_batch* batch) {
+  if (batch) {
+    cudaSetDevice(batch->device);
+    delete batch;
+  }
+  return TSN_OK;
+}
+
+tsn_status tsn_batch_cg_sense(tsn_batch* batch, const void* const* y, const void* const* smaps,
+                              const float* const* density, float lambda, float operator_scale, int32_t iters,
+                              void* const* x, tsn_cg_status* statuses, tsn_stream_t stream) {
+  try {
+    if (!batch || !y || !smaps || !x) fail(TSN_ERR_ARG, "NULL argument (y, smaps and x are required)");
+    if (iters < 0 || iters > kMaxCgIter) fail(TSN_ERR_ARG, "iteration count out of range");
+    if (!(operator_scale > 0.0f) || !std::isfinite(lambda)) fail(TSN_ERR_ARG, "invalid operator scale or lambda");
+    const int count = static_cast<int>(batch->plans.size());
+    std::vector<uint64_t> key;
+    key.reserve(4 * count + 4);
+    for (int i = 0; i < count; ++i) {
+      const float* w = density ? density[i] : nullptr;
+      if (!y[i] || !smaps[i] || !x[i]) fail(TSN_ERR_ARG, "NULL per-case pointer (y, smaps and x are required)");
+      need_aligned({y[i], smaps[i], x[i]});
+      if (reinterpret_cast<uintptr_t>(w) & 3u) fail(TSN_ERR_ARG, "density must be 4-byte aligned");
+      for (const void* q : {y[i], smaps[i], static_cast<const void*>(w), static_cast<const void*>(x[i])})
+        key.push_back(static_cast<uint64_t>(reinterpret_cast<uintptr_t>(q)));
+    }
+    uint32_t lam_bits = 0, scale_bits = 0;
+    std::memcpy(&lam_bits, &lambda, 4);
+    std::memcpy(&scale_bits, &operator_scale, 4);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    key.push_back(static_cast<uint64_t>(iters));
+    key.push_back((static_cast<uint64_t>(lam_bits) << 32) | scale_bits);
+    key.push_back(static_cast<uint64_t>(reinterpret_cast<uintptr_t>(s)));
+    CUDA_OK(cudaSetDevice(batch->device));
+    auto it = batch->graphs.find(key);
+    if (it == batch->graphs.end()) {
+      cudaStream_t cap = s;
+      bool own = false;
+      if (cap == nullptr) {  // the legacy stream cannot be captured: capture on a private stream
+        CUDA_OK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        own = true;
       }
-      if (!host.finite_ok || !std::isfinite(host.rho[iters])) fail(TSN_ERR_NONFINITE, "CG produced non-finite values");
-      if (!host.curvature_ok) fail(TSN_ERR_CURVATURE, "CG denominator <= 0 (positive_curvature = 0)");
+      cudaGraph_t g = nullptr;
+      CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
+      // fork every side stream off the capture, run each case on its stream, join back
+      cudaEventRecord(batch->fork, cap);
+      for (int k = 0; k < batch->streams; ++k) cudaStreamWaitEvent(batch->side[k], batch->fork, 0);
+      for (int i = 0; i < count; ++i)
+        enqueue_cg(batch->plans[i], y[i], smaps[i], density ? density[i] : nullptr, lambda, operator_scale, iters,
+                   x[i], batch->side[batch->lane[i]], batch->streams);
+      for (int k = 0; k < batch->streams; ++k) {
+        cudaEventRecord(batch->join[k], batch->side[k]);
+        cudaStreamWaitEvent(cap, batch->join[k], 0);
+      }
+      const cudaError_t launch_err = cudaGetLastError();
+      const cudaError_t end_err = cudaStreamEndCapture(cap, &g);
+      if (own) cudaStreamDestroy(cap);
+      if (launch_err != cudaSuccess) fail(TSN_ERR_CUDA, cudaGetErrorString(launch_err));
+      if (end_err != cudaSuccess) fail(TSN_ERR_CUDA, cudaGetErrorString(end_err));
+      cudaGraphExec_t exec = nullptr;
+      const cudaError_t inst = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      if (inst != cudaSuccess) fail(TSN_ERR_CUDA, cudaGetErrorString(inst));
+      if (batch->graphs.size() >= 4) {
+        cudaGraphExecDestroy(batch->graphs.begin()->second);
+        batch->graphs.erase(batch->graphs.begin());
+      }
+      it = batch->graphs.emplace(key, exec).first;
+    }
+    CUDA_OK(cudaGraphLaunch(it->second, s));
+    if (statuses) {
+      tsn_status first = TSN_OK;
+      int bad = -1;
+      for (int i = 0; i < count; ++i) {
+        const tsn_status rc = read_cg_state(batch->plans[i], iters, nullptr, &statuses[i], s);
+        if (rc != TSN_OK && first == TSN_OK) {
+          first = rc;
+          bad = i;
+        }
+      }
+      if (first != TSN_OK)
+        fail(first, "batch case " + std::to_string(bad) +
+                        (first == TSN_ERR_NONFINITE ? ": CG produced non-finite values"
+                                                    : ": CG denominator <= 0 (positive_curvature = 0)"));
     }
     return TSN_OK;
   } catch (const std::exception& e) {

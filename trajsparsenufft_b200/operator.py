@@ -221,6 +221,75 @@ class Plan:
         return out
 
 
+class Batch:
+    """Independent plans solved together (tsn_batch_*): one CUDA graph forks the cases over
+    `streams` streams and each case's persistent launches use a 1/streams slice of the GPU.
+
+    The plans stay owned by the caller and must outlive the batch."""
+
+    def __init__(self, plans, streams: int = 0):
+        self.plans = list(plans)
+        if not self.plans:
+            raise ValueError("a batch needs at least one plan")
+        arr = (C.c_void_p * len(self.plans))(*[pl._h.value for pl in self.plans])
+        h = C.c_void_p()
+        check(lib().tsn_batch_create(arr, len(self.plans), int(streams), C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().tsn_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def cg_sense(self, ys, smaps, *, densities=None, lam=1e-4, iters=10, operator_scale=1.0, outs=None,
+                 stream=None, sync=True):
+        """CG-SENSE of every case; returns (list of x, list of status dicts or None).
+
+        A case whose solve went non-finite or lost positive curvature is reported in its
+        status (key "failure"); its x is returned as computed."""
+        torch = _torch()
+        cf = torch.complex64
+        n_cases = len(self.plans)
+        if len(ys) != n_cases or len(smaps) != n_cases:
+            raise ValueError("one y and one smaps per case")
+        if outs is None:
+            outs = [torch.empty((pl.im_size, pl.im_size), dtype=cf, device=y.device) for pl, y in zip(self.plans, ys)]
+        yp, sp, dp, xp = [], [], [], []
+        for i, pl in enumerate(self.plans):
+            n = pl.im_size
+            yp.append(_dev_ptr(ys[i], cf, (pl.coils, pl.samples), f"ys[{i}]").value)
+            sp.append(_dev_ptr(smaps[i], cf, (pl.coils, n, n), f"smaps[{i}]").value)
+            w = None if densities is None else densities[i]
+            dp.append(None if w is None else _dev_ptr(w, torch.float32, (pl.samples,), f"densities[{i}]").value)
+            xp.append(_dev_ptr(outs[i], cf, (n, n), f"outs[{i}]").value)
+        arr = lambda v: (C.c_void_p * n_cases)(*v)
+        st = (CgStatus * n_cases)() if sync else None
+        rc = lib().tsn_batch_cg_sense(self._h, arr(yp), arr(sp), arr(dp), float(lam), float(operator_scale),
+                                      int(iters), arr(xp), st, _stream_handle(stream))
+        statuses = None
+        if sync:
+            statuses = []
+            for s_ in st:
+                d = {"completed_iterations": s_.completed_iterations,
+                     "positive_curvature": bool(s_.positive_curvature), "finite": bool(s_.finite),
+                     "timeout": bool(s_.timeout), "residual0": s_.residual0, "residual_final": s_.residual_final}
+                if not d["finite"]:
+                    d["failure"] = "NONFINITE"
+                elif not d["positive_curvature"]:
+                    d["failure"] = "CURVATURE"
+                statuses.append(d)
+            if rc in (4, 5):
+                return outs, statuses
+        check(rc)
+        return outs, statuses
+
+
 def load_runtime_dir(directory, coils: int, im_size: int, samples: int) -> dict:
     """Runtime inputs in the reference layout (export_real_runtime_inputs.py:97-113)."""
     d = Path(directory)

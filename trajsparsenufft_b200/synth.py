@@ -102,3 +102,26 @@ def add_noise(samples: np.ndarray, seed: int, level: float = 1e-3) -> np.ndarray
     rms = math.sqrt(float(np.mean(np.abs(samples.astype(np.complex128)) ** 2)))
     noise = rng.standard_normal(samples.shape) + 1j * rng.standard_normal(samples.shape)
     return (samples + level * rms / math.sqrt(2.0) * noise).astype(np.complex64)
+
+
+def uneven_batch(count: int = 48, seed: int = BASE_SEED) -> list[dict]:
+    """Seeded uneven batch: image size N from {128, 192, 256, 320} (grid 2N), coils from
+    {4, 8, 12, 16}; even cases golden-angle radial (64-384 spokes x 2N samples), odd cases
+    variable-density spirals (8-32 interleaves x 2048-4096 samples, density exponent 1.5).
+    Case i uses seed + i for its phantom, coils and noise."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for i in range(count):
+        n = int(rng.choice([128, 192, 256, 320]))
+        c = int(rng.choice([4, 8, 12, 16]))
+        if i % 2 == 0:
+            spokes = int(rng.integers(64, 385))
+            traj = golden_radial(spokes, 2 * n)
+            kind = f"radial {spokes}x{2 * n}"
+        else:
+            inter = int(rng.integers(8, 33))
+            samples = int(rng.integers(2048, 4097))
+            traj = vd_spiral(inter, samples, 1.5)
+            kind = f"spiral {inter}x{samples}"
+        cases.append({"n": n, "g": 2 * n, "c": c, "trajectory": traj, "kind": kind, "seed": seed + i})
+    return cases
