@@ -1,0 +1,225 @@
+"""Differentiable NUFFT forward / adjoint and unrolled CG-SENSE (torch.autograd.Function).
+
+The operator pieces come from a `CoilOps` object: the coil-wise NUFFT F (coil images
+[C][N][N] -> samples [C][M]) and its adjoint F^H, both linear.  `PlanOps` serves them from a
+GPU plan (tsn_forward / tsn_adjoint with smaps = NULL); any object with the same two methods
+works (the CPU tests use a dense FP64 matrix).  With S the coil maps, W the density weights
+and G = F^H W F coil by coil:
+
+    A x      = F(S x)                       forward
+    A^H y    = sum_c conj(S_c) F^H(y_c)     adjoint
+    M p      = sum_c conj(S_c) G(S_c p) + lam p
+
+Gradients follow PyTorch's complex convention (dL = Re<grad, dz>).  For w = S u (linear in
+S) the map gradient is grad_w conj(u); for w = conj(S) u it is conj(grad_w) u.
+
+The unrolled solve is the reference's CG (launch_cg, nufft_fp16x2_cg_bench.cu:241-268;
+reference_sparse_solver.py cg_sense) from an initial image x0:
+    r0 = A^H W y - M x0,  p0 = r0,  rho_k = |r_k|^2
+    q = M p, alpha = rho / Re<p, q>, x += alpha p, r -= alpha q, beta = rho'/rho, p = r + beta p.
+Backward runs the adjoint recurrences of these steps in reverse, restarting each segment from
+a checkpoint (x, r, p, rho) stored every `checkpoint` iterations, and returns gradients for
+the k-space data y, the coil maps and x0.  Each reverse step applies G twice per coil (the
+recomputed forward step and the adjoint of q = M p, which also yields the coil-map term).
+"""
+
+from __future__ import annotations
+
+import torch
+
+
+class PlanOps:
+    """Coil-wise NUFFT pieces from a GPU plan (FP16x2 sparse interpolation, FP32 FFTs)."""
+
+    def __init__(self, plan):
+        self.plan = plan
+
+    def forward_coils(self, coil_images: torch.Tensor) -> torch.Tensor:
+        return self.plan.forward(coil_images.contiguous())
+
+    def adjoint_coils(self, y: torch.Tensor) -> torch.Tensor:
+        return self.plan.adjoint(y.contiguous())
+
+
+def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    """Re <a, b> in FP64 (a 0-d tensor)."""
+    return torch.vdot(a.reshape(-1), b.reshape(-1)).real.to(torch.float64)
+
+
+class _Sense:
+    """SENSE algebra over a CoilOps object (no autograd inside)."""
+
+    def __init__(self, ops, smaps, density, lam):
+        self.ops, self.s, self.w, self.lam = ops, smaps, density, lam
+
+    def weigh(self, y):
+        return y if self.w is None else y * self.w
+
+    def G(self, coils):
+        return self.ops.adjoint_coils(self.weigh(self.ops.forward_coils(coils)))
+
+    def combine(self, coils):
+        return (self.s.conj() * coils).sum(0)
+
+    def M(self, p):
+        return self.combine(self.G(self.s * p)) + self.lam * p
+
+    def M_coils(self, p):
+        """(M p, the coil images G(S p)) — the second feeds the coil-map gradient."""
+        t = self.G(self.s * p)
+        return self.combine(t) + self.lam * p, t
+
+
+class NufftForward(torch.autograd.Function):
+    """y = A x = F(S x)."""
+
+    @staticmethod
+    def forward(ctx, x, smaps, ops):
+        ctx.save_for_backward(x, smaps)
+        ctx.ops = ops
+        return ops.forward_coils(smaps * x)
+
+    @staticmethod
+    def backward(ctx, gy):
+        x, smaps = ctx.saved_tensors
+        u = ctx.ops.adjoint_coils(gy)
+        gx = (smaps.conj() * u).sum(0) if ctx.needs_input_grad[0] else None
+        gs = u * x.conj() if ctx.needs_input_grad[1] else None
+        return gx, gs, None
+
+
+class NufftAdjoint(torch.autograd.Function):
+    """x = A^H y = sum_c conj(S_c) F^H(y_c)."""
+
+    @staticmethod
+    def forward(ctx, y, smaps, ops):
+        u = ops.adjoint_coils(y)
+        ctx.save_for_backward(smaps, u)
+        ctx.ops = ops
+        return (smaps.conj() * u).sum(0)
+
+    @staticmethod
+    def backward(ctx, gx):
+        smaps, u = ctx.saved_tensors
+        gy = ctx.ops.forward_coils(smaps * gx) if ctx.needs_input_grad[0] else None
+        gs = gx.conj() * u if ctx.needs_input_grad[1] else None
+        return gy, gs, None
+
+
+def nufft_forward(x, smaps, ops):
+    return NufftForward.apply(x, smaps, ops)
+
+
+def nufft_adjoint(y, smaps, ops):
+    return NufftAdjoint.apply(y, smaps, ops)
+
+
+class UnrolledCgSense(torch.autograd.Function):
+    """x_K of `iters` CG-SENSE iterations from x0; differentiable in y, smaps and x0."""
+
+    @staticmethod
+    def forward(ctx, y, smaps, x0, density, ops, lam, iters, checkpoint):
+        S = _Sense(ops, smaps, density, lam)
+        u = ops.adjoint_coils(S.weigh(y))          # F^H W y, coil images
+        b = S.combine(u)
+        x0_zero = not bool(x0.abs().amax() > 0)
+        x = x0.clone()
+        r = b.clone() if x0_zero else b - S.M(x0)
+        p = r.clone()
+        rho = _rdot(r, r)
+        cps = [(x, r, p, rho)]
+        for k in range(iters):
+            q = S.M(p)
+            alpha = rho / _rdot(p, q)
+            x = x + alpha * p
+            r = r - alpha * q
+            rho_n = _rdot(r, r)
+            p = r + (rho_n / rho) * p
+            rho = rho_n
+            if (k + 1) % checkpoint == 0 and k + 1 < iters:
+                cps.append((x, r, p, rho))
+        ctx.ops, ctx.lam, ctx.iters, ctx.checkpoint, ctx.x0_zero = ops, lam, iters, checkpoint, x0_zero
+        ctx.has_density = density is not None
+        flat = [t for cp in cps for t in cp]
+        ctx.save_for_backward(smaps, x0, u, *(() if density is None else (density,)), *flat)
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        saved = ctx.saved_tensors
+        smaps, x0, u = saved[0], saved[1], saved[2]
+        density = saved[3] if ctx.has_density else None
+        flat = saved[4 if ctx.has_density else 3:]
+        cps = [tuple(flat[i:i + 4]) for i in range(0, len(flat), 4)]
+        S = _Sense(ctx.ops, smaps, density, ctx.lam)
+        need_y, need_s, need_x0 = ctx.needs_input_grad[0], ctx.needs_input_grad[1], ctx.needs_input_grad[2]
+        c, iters = ctx.checkpoint, ctx.iters
+        xb = gx
+        rb = torch.zeros_like(gx)
+        pb = torch.zeros_like(gx)
+        rhob = torch.zeros((), dtype=torch.float64, device=gx.device)
+        sb = torch.zeros_like(smaps) if need_s else None
+        for seg in reversed(range(len(cps))):
+            k0, k1 = seg * c, min(seg * c + c, iters)
+            _, r, p, rho = cps[seg]
+            steps = []
+            for _k in range(k0, k1):  # recompute this segment's forward states
+                if need_s:
+                    q, t = S.M_coils(p)
+                else:
+                    q, t = S.M(p), None
+                gamma = _rdot(p, q)
+                alpha = rho / gamma
+                r_n = r - alpha * q
+                rho_n = _rdot(r_n, r_n)
+                beta = rho_n / rho
+                steps.append((p, q, t, r_n, rho, rho_n, gamma, alpha, beta))
+                p = r_n + beta * p
+                r, rho = r_n, rho_n
+            for p, q, t, r_n, rho, rho_n, gamma, alpha, beta in reversed(steps):
+                rb = rb + pb                                   # p' = r' + beta p
+                betab = _rdot(pb, p)
+                pbk = beta * pb
+                rhob_n = rhob + betab / rho                    # beta = rho' / rho
+                rhobk = -betab * rho_n / (rho * rho)
+                rb = rb + (2.0 * rhob_n) * r_n                 # rho' = |r'|^2
+                qb = -alpha * rb                               # r' = r - alpha q
+                alphab = -_rdot(rb, q)
+                pbk = pbk + alpha * xb                         # x' = x + alpha p
+                alphab = alphab + _rdot(xb, p)
+                rhobk = rhobk + alphab / gamma                 # alpha = rho / gamma
+                gammab = -alphab * rho / (gamma * gamma)
+                pbk = pbk + gammab * q                         # gamma = Re <p, q>
+                qb = qb + gammab * p
+                if need_s:                                     # q = M p (M Hermitian)
+                    mqb, tb = S.M_coils(qb)
+                    sb = sb + qb.conj() * t + tb * p.conj()
+                else:
+                    mqb = S.M(qb)
+                pb = pbk + mqb
+                rhob = rhobk
+        # p0 = r0, rho0 = |r0|^2, r0 = b - M x0
+        r0 = cps[0][1]
+        rb = rb + pb + (2.0 * rhob) * r0
+        gy = gs = gx0 = None
+        if need_x0:
+            gx0 = xb - S.M(rb)                                # x0 directly and through r0 = b - M x0
+        if need_s:
+            if not ctx.x0_zero:                               # the - M x0 term, cotangent -rb
+                v = -rb
+                sb = sb + v.conj() * S.G(smaps * x0) + S.G(smaps * v) * x0.conj()
+            sb = sb + rb.conj() * u                           # b = sum conj(S) F^H W y
+            gs = sb
+        if need_y:
+            gy = S.weigh(ctx.ops.forward_coils(smaps * rb))
+        return gy, gs, gx0, None, None, None, None, None
+
+
+def cg_sense(y, smaps, ops, *, x0=None, density=None, lam=1e-4, iters=10, checkpoint=2):
+    """Differentiable unrolled CG-SENSE: x after `iters` iterations of (A^H W A + lam) x = A^H W y
+    from x0 (zero by default), with CG states checkpointed every `checkpoint` iterations."""
+    if x0 is None:
+        x0 = torch.zeros(smaps.shape[1:], dtype=smaps.dtype, device=smaps.device)
+    if checkpoint < 1:
+        raise ValueError("checkpoint interval must be >= 1")
+    return UnrolledCgSense.apply(y, smaps, x0, density, ops, float(lam), int(iters), int(checkpoint))
