@@ -9,10 +9,12 @@ phantoms / coil maps / trajectories (the reference measures on OCMR, which is no
 available); the measurement is the operator applied to the phantom plus 1e-3 rms noise.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config headline|cfg0|batch48]
+                    [--config headline|cfg0|batch48|grad4]
 
 --config batch48 reconstructs a seeded uneven batch of 48 cases per step through the batched
 graph and reports the plain per-case drop-in (one solve after another) beside it.
+--config grad4 times differentiable unrolled reconstructions (forward + hand-written backward,
+gradients w.r.t. k-space data, coil maps and x0) of 4 cases per step.
 
 Multi-GPU (torchrun, one process per GPU) runs independent replicas: every rank
 reconstructs its own frames with no collective on the data path; value = all ranks'
@@ -41,7 +43,9 @@ METRIC = "CG-SENSE recons/s 256²x8coil x10CG at NRMSE<=0.2% vs FP64: batched/gr
 CONFIGS = {
     "headline": dict(n=256, g=512, c=8, spokes=256, readout=512, width=6, iters=10, density=False),
     "cfg0": dict(n=128, g=256, c=4, spokes=96, readout=256, width=6, iters=10, density=True),
-    "batch48": dict(batch=True, cases=48, streams=8, width=6, iters=10),
+    "batch48": dict(batch=True, cases=48, streams=4, width=6, iters=10),
+    "grad4": dict(grad=True, cases=4, n=256, g=512, c=8, spokes=128, readout=512, width=6, iters=10, checkpoint=2,
+                  density=False),
 }
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
@@ -481,6 +485,155 @@ def run_batch(args, cfg) -> dict | None:
     return out if rank == 0 else None
 
 
+def run_grad(args, cfg) -> dict | None:
+    """Differentiable unrolled reconstructions: loss = sum_i |x_i - x_true_i|^2 after 10 CG-SENSE
+    iterations of each case, gradients w.r.t. k-space data, coil maps and x0 (autograd.py)."""
+    import torch
+    from trajsparsenufft_b200 import autograd as tad
+    from trajsparsenufft_b200 import synth
+    from trajsparsenufft_b200.operator import Plan
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    n, g, c = cfg["n"], cfg["g"], cfg["c"]
+    traj = synth.golden_radial(cfg["spokes"], cfg["readout"])
+    plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=cfg["width"], device=local)
+    ops = tad.PlanOps(plan)
+    iters, lam, every = cfg["iters"], 1e-4, cfg["checkpoint"]
+    xts, maps, ys = [], [], []
+    for i in range(cfg["cases"]):
+        seed = 20260823 + 100 * rank + i
+        xt = torch.from_numpy(synth.ellipse_phantom(n, seed)).to(dev)
+        s = torch.from_numpy(synth.coil_maps(n, c, seed)).to(dev)
+        yc = plan.forward(xt, s)
+        gen = torch.Generator(device=dev).manual_seed(seed)
+        rms = yc.abs().pow(2).mean().sqrt()
+        noise = torch.complex(torch.randn(yc.shape, device=dev, generator=gen),
+                              torch.randn(yc.shape, device=dev, generator=gen))
+        ys.append((yc + noise * (1e-3 * rms / math.sqrt(2.0))).contiguous())
+        xts.append(xt)
+        maps.append(s)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    outs = [torch.empty((n, n), dtype=torch.complex64, device=dev) for _ in ys]
+
+    def grad_step(y_in=None, s_in=None):
+        y_in = ys if y_in is None else y_in
+        s_in = maps if s_in is None else s_in
+        leaves = []
+        loss = 0.0
+        for y, s, xt in zip(y_in, s_in, xts):
+            yl = y.detach().requires_grad_(True)
+            sl = s.detach().requires_grad_(True)
+            x0 = torch.zeros((n, n), dtype=torch.complex64, device=dev, requires_grad=True)
+            xk = tad.cg_sense(yl, sl, ops, x0=x0, lam=lam, iters=iters, checkpoint=every)
+            loss = loss + (xk - xt).abs().pow(2).sum()
+            leaves.append((yl, sl, x0))
+        loss.backward()
+        return loss, leaves
+
+    def fwd_step():
+        with torch.no_grad():
+            for y, s in zip(ys, maps):
+                tad.cg_sense(y, s, ops, lam=lam, iters=iters, checkpoint=every)
+
+    def plain_step():
+        for y, s, o in zip(ys, maps, outs):
+            plan.cg_sense(y, s, lam=lam, iters=iters, out=o, sync=False)
+
+    def timed(step):
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+        torch.cuda.synchronize()
+        st = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        en = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            st[k].record()
+            step()
+            en[k].record()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in zip(st, en))
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    with ClockSampler(local) as clocks:
+        grad_ms = timed(grad_step)
+    fwd_ms = timed(fwd_step)
+    plain_ms = timed(plain_step)
+
+    # end to end: inputs from pinned host memory, loss and all gradients back to the host
+    y_h = [y.cpu().pin_memory() for y in ys]
+    s_h = [s.cpu().pin_memory() for s in maps]
+
+    def e2e_step():
+        y_d = [h.to(dev, non_blocking=True) for h in y_h]
+        s_d = [h.to(dev, non_blocking=True) for h in s_h]
+        loss, leaves = grad_step(y_d, s_d)
+        host = [loss.detach().to("cpu", non_blocking=True)]
+        for yl, sl, x0 in leaves:
+            host += [yl.grad.to("cpu", non_blocking=True), sl.grad.to("cpu", non_blocking=True),
+                     x0.grad.to("cpu", non_blocking=True)]
+        return host
+
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    es = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    for k in range(e2e_steps):
+        flush.zero_()
+        es[k].record()
+        e2e_step()
+        ee[k].record()
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(es, ee))
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.destroy_process_group()
+    cases = cfg["cases"]
+    value = world * cases * args.steps / (grad_ms / 1e3)
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "recons/s (with gradients)", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(grad_ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16x2->f32 (f64 CG scalars)",
+        "data": "synthetic",
+        "config": {"workload": f"{cases} cases per step: {n}x{n} image, {g}x{g} grid, {c} coils, golden-angle "
+                               f"radial {cfg['spokes']}x{cfg['readout']}, KB J={cfg['width']}, {iters} unrolled "
+                               f"CG-SENSE iterations (checkpoint every {every}); loss |x - x_true|^2, gradients "
+                               "w.r.t. k-space data, coil maps and x0",
+                   "recons_per_step": cases, "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "forward_only": {"value": round(world * cases * args.steps / (fwd_ms / 1e3), 3), "unit": "recons/s",
+                         "ms_per_step": round(fwd_ms / args.steps, 4)},
+        "backward_over_forward": round((grad_ms - fwd_ms) / fwd_ms, 3),
+        "plain_graph_solver": {"value": round(world * cases * args.steps / (plain_ms / 1e3), 3),
+                               "unit": "recons/s", "ms_per_step": round(plain_ms / args.steps, 4)},
+        "e2e": {"value": round(world * cases * e2e_steps / (float(te.item()) / 1e3), 3),
+                "unit": "recons/s (with gradients)",
+                "h2d_bytes_per_step": int(sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)),
+                "d2h_bytes_per_step": int(8 + sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)
+                                          + cases * n * n * 8)},
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    return out if rank == 0 else None
+
+
 def run_reference(args, cfg) -> dict | None:
     """Reference arm: the reference's CPU FP32 CG-SENSE path (restated port) on host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -531,14 +684,19 @@ def main() -> int:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", choices=tuple(CONFIGS), default="headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--streams", type=int, default=0, help="batch48: concurrent case streams (default 4)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.streams > 0:
+        cfg["streams"] = args.streams
     if args.impl == "reference":
         out = run_reference(args, cfg)
     elif cfg.get("batch"):
         out = run_batch(args, cfg)
+    elif cfg.get("grad"):
+        out = run_grad(args, cfg)
     else:
         out = run_ours(args, cfg)
     if out is not None:
