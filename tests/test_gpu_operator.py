@@ -162,3 +162,22 @@ def test_misaligned_device_arrays_are_rejected():
     assert info.value.kind == "ARG"
     y = plan.forward(xt, st)  # the plan stays usable
     assert torch.isfinite(torch.view_as_real(y)).all()
+
+
+@pytest.mark.parametrize("iters", [20, 50])
+def test_long_cg_stays_on_the_fp64_path(iters):
+    """Long CG (the reference's long-CG stability check, tools/check_long_cg.py:11-27): at 20 and
+    50 iterations the FP16x2 solve stays finite with positive curvature and its image matches
+    the FP64 CG at the same iteration count within the 0.2% magnitude NRMSE gate."""
+    name = "cfg0"
+    traj, x, s, n, g, c, j, readout = case(name)
+    plan = _plan(name)
+    _, st, yt = torch_inputs(name)
+    from trajsparsenufft_b200 import synth
+    w = synth.ramp_density(traj, readout)
+    x_gpu, hist, status = plan.cg_sense(yt, st, density=torch.from_numpy(w).cuda(), lam=1e-4, iters=iters)
+    assert status["positive_curvature"] and status["finite"] and status["completed_iterations"] == iters
+    assert np.all(np.isfinite(hist)) and hist[-1] < hist[0]
+    nd = onudft.Nudft(traj, n)
+    x_ref, _, _ = oracle_cg(lambda v: nd.forward(v, s), lambda v: nd.adjoint(v, s), measurement(name), w, iters, 1e-4)
+    assert oop.magnitude_nrmse(x_gpu.cpu().numpy(), x_ref) <= 2e-3
