@@ -9,8 +9,10 @@
 namespace tsn {
 namespace dev {
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add / subtract as one paired FP32 instruction (sm_100 FADD2; each lane rounds
+// exactly like the scalar add).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -80,6 +82,16 @@ __device__ __forceinline__ void split_hi_res(float v, __half& hi, __half& res) {
 
 __device__ __forceinline__ uint32_t pack_half2(__half lo, __half hi) {
   return static_cast<uint32_t>(__half_as_ushort(lo)) | (static_cast<uint32_t>(__half_as_ushort(hi)) << 16);
+}
+
+// Complex (re, im) -> packed FP16 high parts (re low, im high) and packed FP16 residuals:
+// split_hi_res on each component, with the paired conversions (same rounding, same bits).
+__device__ __forceinline__ void split_hi_res2(float re, float im, uint32_t& hi, uint32_t& res) {
+  const __half2 h = __floats2half2_rn(re, im);
+  const float2 back = __half22float2(h);
+  const __half2 r = __floats2half2_rn(re - back.x, im - back.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  res = *reinterpret_cast<const uint32_t*>(&r);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

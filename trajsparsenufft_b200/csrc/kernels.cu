@@ -152,12 +152,11 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
         } else if constexpr (EPI == EPI_GRID) {
           o.c64[static_cast<size_t>(row) * C + coil] = make_float2(re, im);
         } else {
-          __half hr_, rr_, hi_, ri_;
-          split_hi_res(re, hr_, rr_);
-          split_hi_res(im, hi_, ri_);
+          uint32_t hw, rw;
+          split_hi_res2(re, im, hw, rw);
           uint32_t* rowp = reinterpret_cast<uint32_t*>(o.panel + static_cast<size_t>(row) * ROWH);
-          rowp[coil] = pack_half2(hr_, hi_);
-          rowp[C + coil] = pack_half2(rr_, ri_);
+          rowp[coil] = hw;
+          rowp[C + coil] = rw;
         }
       }
     }
@@ -418,13 +417,12 @@ __device__ __forceinline__ int slab_swz(int n, int chn) {
 __device__ __forceinline__ int slab_idx(int n, int c, int C) {
   return n * C + 2 * ((c >> 1) ^ slab_swz(n, C >> 1)) + (c & 1);
 }
-// copy `rows` contiguous rows of C complex values into a swizzled slab (all threads)
+// copy `rows` contiguous rows of C complex values into a swizzled slab (all threads; the
+// block has 32*C threads, so every thread keeps one 16-byte chunk column, 64 rows apart)
 __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, int rows, int C) {
   const int chn = C >> 1;
-  for (int q = threadIdx.x; q < rows * chn; q += blockDim.x) {
-    const int n = q / chn, k = q - n * chn;
-    cp_async16(dst + n * C + 2 * (k ^ slab_swz(n, chn)), src + n * C + 2 * k);
-  }
+  const int k = threadIdx.x % chn;
+  for (int n = threadIdx.x / chn; n < rows; n += 64) cp_async16(dst + n * C + 2 * (k ^ slab_swz(n, chn)), src + n * C + 2 * k);
 }
 
 // The four FFT stages run one warp per coil in CTAs of 32*C threads (C <= MAXW). With
@@ -568,6 +566,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_cols_kernel(FftArgs f, const float2*
   const int ch2 = C >> 1;  // 16-byte chunks per panel row
   const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
   const int c = warp;
+  const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane + f.shift, C >> 1)) + (c & 1);
   int it = 0;
   for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, ++it) {
     const int b = nbuf == 2 ? (it & 1) : 0;
@@ -586,7 +585,9 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_cols_kernel(FftArgs f, const float2*
       const int n = warp_fft_in_index<G>(j);
       int i0 = n + f.shift;
       if (i0 >= G) i0 -= G;
-      v[j] = i0 < N ? in_s[slab_idx(i0, c, C)] : make_float2(0.f, 0.f);
+      // power-of-two grids: the lane's low five index bits (and so its swizzle) are fixed
+      const int idx = FftPlan<G>::R == 1 ? i0 * C + lane_off : slab_idx(i0, c, C);
+      v[j] = i0 < N ? in_s[idx] : make_float2(0.f, 0.f);
     }
     __syncthreads();  // slab consumed
     warp_fft<G, false>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
@@ -595,11 +596,10 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_cols_kernel(FftArgs f, const float2*
 #pragma unroll
     for (int m = 0; m < P; ++m) {
       const int q0 = warp_fft_out_index<G>(m);
-      __half hr, rr, hi, ri;
-      split_hi_res(v[m].x, hr, rr);
-      split_hi_res(v[m].y, hi, ri);
-      out_s[q0 * OP + c] = pack_half2(hr, hi);
-      out_s[q0 * OP + C + c] = pack_half2(rr, ri);
+      uint32_t hw, rw;
+      split_hi_res2(v[m].x, v[m].y, hw, rw);
+      out_s[q0 * OP + c] = hw;
+      out_s[q0 * OP + C + c] = rw;
     }
     __syncthreads();
     uint32_t* dst = reinterpret_cast<uint32_t*>(panel + static_cast<size_t>(q1) * G * 4 * C);
@@ -635,11 +635,7 @@ __global__ void split_samples_kernel(const float2* __restrict__ y, const float* 
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const float2 val = y[static_cast<size_t>(4 * q + k) * m + row];
-      __half hr, rr, hi_, ri;
-      split_hi_res(val.x * w, hr, rr);
-      split_hi_res(val.y * w, hi_, ri);
-      hi[k] = pack_half2(hr, hi_);
-      res[k] = pack_half2(rr, ri);
+      split_hi_res2(val.x * w, val.y * w, hi[k], res[k]);
     }
     *reinterpret_cast<uint4*>(pu + row * 2 * C + 4 * q) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *reinterpret_cast<uint4*>(pu + row * 2 * C + C + 4 * q) = make_uint4(res[0], res[1], res[2], res[3]);
@@ -668,6 +664,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_cols_kernel(FftArgs f, const float2*
   const int ch2 = C >> 1;  // 16-byte chunks per output row
   const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
   const int c = warp;
+  const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
   int it = 0;
   for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, ++it) {
     const int b = nbuf == 2 ? (it & 1) : 0;
@@ -682,7 +679,10 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_cols_kernel(FftArgs f, const float2*
     const float2* in_s = reinterpret_cast<const float2*>(reg);
     float2 v[P];
 #pragma unroll
-    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(warp_fft_in_index<G>(j), c, C)];
+    for (int j = 0; j < P; ++j) {
+      const int n = warp_fft_in_index<G>(j);
+      v[j] = in_s[FftPlan<G>::R == 1 ? n * C + lane_off : slab_idx(n, c, C)];
+    }
     __syncthreads();
     warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
     __syncthreads();
@@ -729,10 +729,9 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2*
     float2* dst = reinterpret_cast<float2*>(reg);
     // G runs of C complex values (8C bytes each, 16-byte aligned for even C), swizzled
     const int chn = C / 2;
-    for (int e = threadIdx.x; e < G * chn; e += blockDim.x) {
-      const int q1 = e / chn, k = e - q1 * chn;
+    const int k = threadIdx.x % chn;  // 32*C threads: 64 rows per pass
+    for (int q1 = threadIdx.x / chn; q1 < G; q1 += 64)
       cp_async16(dst + q1 * C + 2 * (k ^ slab_swz(q1, chn)), w1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * k);
-    }
     if (epi_smem) {
       const size_t off = static_cast<size_t>(i0) * N;
       if (f.smaps)
@@ -748,6 +747,7 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2*
   if (mode == 2) factor = static_cast<float>(G) / st->sigma[iter] * inv_scale2;
   else factor = inv_scale2 / st->sigma_y;
   const int c = warp;
+  const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
   for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x) {
     if (i0 != blockIdx.x) {
       __syncthreads();
@@ -758,7 +758,10 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2*
     const float2* in_s = reinterpret_cast<const float2*>(reg);
     float2 v[P];
 #pragma unroll
-    for (int j = 0; j < P; ++j) v[j] = in_s[slab_idx(warp_fft_in_index<G>(j), c, C)];
+    for (int j = 0; j < P; ++j) {
+      const int n = warp_fft_in_index<G>(j);
+      v[j] = in_s[FftPlan<G>::R == 1 ? n * C + lane_off : slab_idx(n, c, C)];
+    }
     __syncthreads();
     warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
     __syncthreads();
