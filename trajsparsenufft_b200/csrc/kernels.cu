@@ -425,12 +425,12 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
   for (int n = threadIdx.x / chn; n < rows; n += 64) cp_async16(dst + n * C + 2 * (k ^ slab_swz(n, chn)), src + n * C + 2 * k);
 }
 
-// The four FFT stages run one warp per coil in CTAs of 32*C threads (C <= MAXW). With
-// MAXW = 8 and G <= 512 the 80-register cap keeps three CTAs resident per SM (two at 128
-// registers for larger grids). The per-warp
-// FFT scratch and the output staging reuse the input slab's shared memory once it is
-// consumed, which keeps a CTA near 72 KB. The column stages double-buffer the slab when two
-// regions fit, so the next item streams in while the current one is transformed.
+// The four FFT stages run one warp per coil in CTAs of 32*C threads (instantiated per coil
+// count). With C <= 8 and G <= 512 the 80-register cap keeps three CTAs resident per SM (two
+// at 128 registers for larger grids). The per-warp FFT scratch and the output staging reuse
+// the input slab's shared memory once it is consumed, which keeps a CTA near 72 KB. The
+// column stages double-buffer the slab when two regions fit, so the next item streams in
+// while the current one is transformed.
 #define TSN_FFT_BOUNDS(G, MAXW) __launch_bounds__((MAXW) * 32, (MAXW) > 8 ? 1 : ((G) <= 512 ? 3 : 2))
 
 // Forward rows (x-stage). Image row i0 -> z1[q1][i0][c] for all q1. Fuses the SENSE
@@ -442,14 +442,15 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
 //     mode 1 (CG):        row0 = r row, row1 = p row, maps = S_c rows
 //   the per-warp FFT scratch [C][SCR], and the output rows [G][C+1] float2.
 // Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844).
-template <int G, int MAXW>
-__global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1,
+template <int G, int CC>
+__global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1,
                                                      int mode, float2* __restrict__ p, const float2* __restrict__ r,
                                                      const double* __restrict__ parts, int nparts,
                                                      CgState* __restrict__ st, int iter) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
-  const int N = f.N, C = f.C;
+  const int N = f.N;
+  constexpr int C = CC;  // coils (one warp each), a compile-time stride
   const int in_f2 = (2 + C) * N;  // float2 of the slab before the scaling row
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
@@ -547,12 +548,13 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_rows_kernel(FftArgs f, const float2*
 // Shared memory: twiddles [G] | nbuf regions of `region` bytes, each holding in turn the
 // swizzled input slab [N][C], the per-warp FFT scratch and the output rows [G][2C+1] words.
 // Reference: fft512_allcoils1_shared16_to_n16 (nufft_custom_fft_forward_bench.cu:538-747).
-template <int G, int MAXW>
-__global__ void TSN_FFT_BOUNDS(G, MAXW) fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1,
+template <int G, int CC>
+__global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_cols_kernel(FftArgs f, const float2* __restrict__ z1,
                                                      __half* __restrict__ panel, int region, int nbuf) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
-  const int N = f.N, C = f.C;
+  const int N = f.N;
+  constexpr int C = CC;  // coils (one warp each), a compile-time stride
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* regs = reinterpret_cast<uint8_t*>(tw_s + G);
   const int OP = 2 * C + 1;
@@ -646,12 +648,13 @@ __global__ void split_samples_kernel(const float2* __restrict__ y, const float* 
 // Shared memory: twiddles [G] | nbuf regions, each holding in turn the swizzled slab [G][C],
 // the per-warp FFT scratch and the cropped output rows [N][C+1] float2.
 // Reference: ifft512_rows8_regular_transposed (nufft_custom_fft_forward_bench.cu:1463-1515).
-template <int G, int MAXW>
-__global__ void TSN_FFT_BOUNDS(G, MAXW) inv_cols_kernel(FftArgs f, const float2* __restrict__ grid,
+template <int G, int CC>
+__global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_cols_kernel(FftArgs f, const float2* __restrict__ grid,
                                                      float2* __restrict__ w1, int region, int nbuf) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
-  const int N = f.N, C = f.C;
+  const int N = f.N;
+  constexpr int C = CC;  // coils (one warp each), a compile-time stride
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* regs = reinterpret_cast<uint8_t*>(tw_s + G);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -709,15 +712,16 @@ __global__ void TSN_FFT_BOUNDS(G, MAXW) inv_cols_kernel(FftArgs f, const float2*
 // scaling row [N] float. Without epi_smem the epilogue reads them from global memory.
 // Reference: ifft512_rows8_regular_crop_scale (nufft_custom_fft_forward_bench.cu:1517-1552)
 // followed by sense_combine_scaled (nufft_fp16x2_cg_bench.cu:27-54).
-template <int G, int MAXW>
-__global__ void TSN_FFT_BOUNDS(G, MAXW) inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2* __restrict__ out,
+template <int G, int CC>
+__global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f, const float2* __restrict__ w1, float2* __restrict__ out,
                                                      int mode, float2* __restrict__ x, float2* __restrict__ r,
                                                      const float2* __restrict__ p, double* __restrict__ parts,
                                                      CgState* __restrict__ st, int iter, float inv_scale2,
                                                      float lambda_scaled, int region, int epi_smem) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
-  const int N = f.N, C = f.C;
+  const int N = f.N;
+  constexpr int C = CC;  // coils (one warp each), a compile-time stride
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
   float2* emaps = reinterpret_cast<float2*>(reg + region);
@@ -944,22 +948,23 @@ static int persistent_grid(K k, int threads, size_t smem, int items, int share =
     case 1024: { constexpr int GG = 1024; __VA_ARGS__; } break; \
     default: break;                                            \
   }
-// FFT stage instantiation by CTA size bound: up to 8 coils (three CTAs per SM) or 16
-#define TSN_FFT_MAXW(C_, ...)                   \
-  if ((C_) <= 8) {                              \
-    constexpr int MW = 8;                       \
-    __VA_ARGS__;                                \
-  } else {                                      \
-    constexpr int MW = 16;                      \
-    __VA_ARGS__;                                \
+// FFT stage instantiation per coil count (4, 8, 12, 16): the index arithmetic folds to
+// constants, and CTAs of up to 8 warps keep three per SM
+#define TSN_FFT_C(C_, ...)                                  \
+  switch (C_) {                                             \
+    case 4: { constexpr int CC = 4; __VA_ARGS__; } break;   \
+    case 8: { constexpr int CC = 8; __VA_ARGS__; } break;   \
+    case 12: { constexpr int CC = 12; __VA_ARGS__; } break; \
+    case 16: { constexpr int CC = 16; __VA_ARGS__; } break; \
+    default: break;                                         \
   }
 
 void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
                      const double* partials, int nparts, CgState* st, int iter, cudaStream_t s) {
   TSN_G_SWITCH(f.G, {
     const size_t sm = sizeof(float2) * GG + fwd_rows_region<GG>(f);
-    TSN_FFT_MAXW(f.C, {
-      auto k = fwd_rows_kernel<GG, MW>;
+    TSN_FFT_C(f.C, {
+      auto k = fwd_rows_kernel<GG, CC>;
       ensure_smem(k, sm);
       const int grid = persistent_grid(k, 32 * f.C, sm, f.N, f.share);
       k<<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
@@ -973,8 +978,8 @@ void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStre
     const size_t base = sizeof(float2) * GG;
     const int nbuf = base + 2 * region <= kFftTwoCtaSmem ? 2 : 1;
     const size_t sm = base + nbuf * region;
-    TSN_FFT_MAXW(f.C, {
-      auto k = fwd_cols_kernel<GG, MW>;
+    TSN_FFT_C(f.C, {
+      auto k = fwd_cols_kernel<GG, CC>;
       ensure_smem(k, sm);
       const int grid = persistent_grid(k, 32 * f.C, sm, f.G, f.share);
       k<<<grid, 32 * f.C, sm, s>>>(f, z1, panel, static_cast<int>(region), nbuf);
@@ -995,8 +1000,8 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
     const size_t base = sizeof(float2) * GG;
     const int nbuf = base + 2 * region <= kFftTwoCtaSmem ? 2 : 1;
     const size_t sm = base + nbuf * region;
-    TSN_FFT_MAXW(f.C, {
-      auto k = inv_cols_kernel<GG, MW>;
+    TSN_FFT_C(f.C, {
+      auto k = inv_cols_kernel<GG, CC>;
       ensure_smem(k, sm);
       const int g = persistent_grid(k, 32 * f.C, sm, f.G, f.share);
       k<<<g, 32 * f.C, sm, s>>>(f, grid, w1, static_cast<int>(region), nbuf);
@@ -1012,8 +1017,8 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
     const size_t epi = inv_rows_epi(f, mode);
     const int epi_smem = base + epi <= kFftTwoCtaSmem ? 1 : 0;
     const size_t sm = base + (epi_smem ? epi : 0);
-    TSN_FFT_MAXW(f.C, {
-      auto k = inv_rows_kernel<GG, MW>;
+    TSN_FFT_C(f.C, {
+      auto k = inv_rows_kernel<GG, CC>;
       ensure_smem(k, sm);
       const int g = persistent_grid(k, 32 * f.C, sm, f.N, f.share);
       k<<<g, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2, lambda_scaled,
