@@ -157,17 +157,24 @@ uint32_t live_columns(const HostView& h, int64_t t) {
   return m;
 }
 
-// Persistent-warp runs: contiguous item runs of about tiles / warps tiles each.
+// Persistent-warp runs: contiguous item runs of about tiles / warps tiles each. Run w ends at
+// the item boundary nearest to (w + 1) * tiles / warps, so no run drifts by more than half an
+// item from the ideal split.
 std::vector<int2> cut_ranges(const std::vector<int64_t>& item_ends, int64_t tiles, int warps) {
-  const int64_t target = std::max<int64_t>(1, (tiles + warps - 1) / std::max(1, warps));
+  warps = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(warps, static_cast<int64_t>(item_ends.size()))));
   std::vector<int2> ranges;
   int64_t run_start = 0;
-  for (int64_t e : item_ends)
-    if (e - run_start >= target) {
-      ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(e)));
-      run_start = e;
-    }
-  if (run_start < tiles) ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(tiles)));
+  size_t i = 0;
+  for (int w = 0; w < warps && run_start < tiles; ++w) {
+    const double ideal = static_cast<double>(tiles) * (w + 1) / warps;
+    while (i + 1 < item_ends.size() && item_ends[i] <= run_start) ++i;  // first boundary after the start
+    while (i + 1 < item_ends.size() &&
+           std::abs(static_cast<double>(item_ends[i + 1]) - ideal) <= std::abs(static_cast<double>(item_ends[i]) - ideal))
+      ++i;
+    const int64_t end = (w + 1 == warps) ? tiles : item_ends[i];
+    ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(end)));
+    run_start = end;
+  }
   return ranges;
 }
 
