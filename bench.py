@@ -118,6 +118,21 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def max_over_ranks(ms: float, device) -> float:
+    """Max of a per-rank device time over all ranks (the slowest replica sets the job time)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, recons_per_step: int, steps: int, max_ms: float) -> float:
+    """Whole-job reconstructions per second: every rank's reconstructions over the max time."""
+    return world * recons_per_step * steps / (max_ms / 1e3)
+
+
 def measured_peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -213,11 +228,8 @@ def run_ours(args, cfg) -> dict:
             dist.barrier()
         wall = time.perf_counter() - wall0
     dev_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms / 1e3)
+    max_ms = max_over_ranks(dev_ms, dev)
+    value = job_rate(world, 1, args.steps, max_ms)
 
     # end to end through the public call with host buffers: every step copies its y and maps
     # from pinned host memory and reads its image back.  The copy of step k+1 runs on a side
@@ -267,10 +279,7 @@ def run_ours(args, cfg) -> dict:
 
     e2e_run(2)
     e2e_ms = e2e_run(e2e_steps)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / (float(te.item()) / 1e3)
+    e2e_value = job_rate(world, 1, e2e_steps, max_over_ranks(e2e_ms, dev))
 
     # dominant kernel: per-stage CUDA-event timing on this stream
     stages = plan.profile_stages(y, smaps, reps=20)
@@ -391,18 +400,14 @@ def run_batch(args, cfg) -> dict | None:
             step()
             en[k].record()
         torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in zip(st, en))
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(st, en)), dev)
 
     plain_ms = timed(plain_step)
     with ClockSampler(local) as clocks:
         batch_ms = timed(batch_step)
     n_cases = len(specs)
-    value = world * n_cases * args.steps / (batch_ms / 1e3)
-    plain_value = world * n_cases * args.steps / (plain_ms / 1e3)
+    value = job_rate(world, n_cases, args.steps, batch_ms)
+    plain_value = job_rate(world, n_cases, args.steps, plain_ms)
 
     # end to end: every step copies all cases' y and maps from pinned host memory (side stream,
     # overlapping the previous step's solve) and reads every image back
@@ -454,11 +459,9 @@ def run_batch(args, cfg) -> dict | None:
     e2e_steps = max(3, args.steps // 2)
     e2e_run(2)
     e2e_ms = e2e_run(e2e_steps)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    e2e_value = job_rate(world, n_cases, e2e_steps, max_over_ranks(e2e_ms, dev))
     if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.destroy_process_group()
-    e2e_value = world * n_cases * e2e_steps / (float(te.item()) / 1e3)
     samples = sum(len(sp["trajectory"]) * sp["c"] for sp in specs)
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "recons/s", "n_gpus": world, "steps": args.steps,
@@ -563,11 +566,7 @@ def run_grad(args, cfg) -> dict | None:
             step()
             en[k].record()
         torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in zip(st, en))
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(st, en)), dev)
 
     with ClockSampler(local) as clocks:
         grad_ms = timed(grad_step)
@@ -600,13 +599,11 @@ def run_grad(args, cfg) -> dict | None:
         e2e_step()
         ee[k].record()
     torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(es, ee))
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    e2e_max_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(es, ee)), dev)
     if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.destroy_process_group()
     cases = cfg["cases"]
-    value = world * cases * args.steps / (grad_ms / 1e3)
+    value = job_rate(world, cases, args.steps, grad_ms)
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "recons/s (with gradients)", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(grad_ms / args.steps, 4),
@@ -618,12 +615,12 @@ def run_grad(args, cfg) -> dict | None:
                                "w.r.t. k-space data, coil maps and x0",
                    "recons_per_step": cases, "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"replicas x{world}"},
-        "forward_only": {"value": round(world * cases * args.steps / (fwd_ms / 1e3), 3), "unit": "recons/s",
+        "forward_only": {"value": round(job_rate(world, cases, args.steps, fwd_ms), 3), "unit": "recons/s",
                          "ms_per_step": round(fwd_ms / args.steps, 4)},
         "backward_over_forward": round((grad_ms - fwd_ms) / fwd_ms, 3),
-        "plain_graph_solver": {"value": round(world * cases * args.steps / (plain_ms / 1e3), 3),
+        "plain_graph_solver": {"value": round(job_rate(world, cases, args.steps, plain_ms), 3),
                                "unit": "recons/s", "ms_per_step": round(plain_ms / args.steps, 4)},
-        "e2e": {"value": round(world * cases * e2e_steps / (float(te.item()) / 1e3), 3),
+        "e2e": {"value": round(job_rate(world, cases, e2e_steps, e2e_max_ms), 3),
                 "unit": "recons/s (with gradients)",
                 "h2d_bytes_per_step": int(sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)),
                 "d2h_bytes_per_step": int(8 + sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)
