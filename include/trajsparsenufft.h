@@ -62,7 +62,9 @@ enum { TSN_POLICY_TRAJECTORY = 0, TSN_POLICY_MORTON = 1, TSN_POLICY_OVERLAP = 2,
 enum { TSN_ILLEGAL_SPLIT24 = 0, TSN_ILLEGAL_CSR_RESIDUAL = 1 };
 /* Views. */
 enum { TSN_VIEW_G = 0, TSN_VIEW_GT = 1 };
-/* Interpolation kernel choice. */
+/* Interpolation kernel choice.  The pack's 16-row groups each carry their own K32 column
+ * set (M_TILE = 16, src/nufft_layout_oracle.py:29); tcgen05.mma needs 64 or 128 rows sharing
+ * one K operand, so TSN_INTERP_TCGEN05 is reserved and refused with TSN_ERR_UNSUPPORTED. */
 enum { TSN_INTERP_AUTO = 0, TSN_INTERP_MMA_SP = 1, TSN_INTERP_TCGEN05 = 2 };
 /* Plan flags. */
 enum {
@@ -94,7 +96,7 @@ typedef struct tsn_plan_info {
   int64_t pack_bytes[2];      /* device bytes of each view's pack              */
   int64_t workspace_bytes;    /* device workspace owned by the plan            */
   double plan_seconds;        /* host planner wall time                        */
-  int32_t interp;             /* kernel actually used (TSN_INTERP_MMA_SP / _TCGEN05) */
+  int32_t interp;             /* kernel actually used (TSN_INTERP_MMA_SP)              */
   int32_t reserved[7];
 } tsn_plan_info;
 
@@ -189,6 +191,21 @@ tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x
 tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const float* density,
                         float lambda, float operator_scale, int32_t iters, void* x,
                         double* residual_history, tsn_cg_status* status, tsn_stream_t stream);
+/* Reliable-update CG (reference_sparse_solver.py:200-332 cg_sense, reliable_update_period and
+ * reliable_update_direction): after every `reliable_update_period`-th iteration except the
+ * last, the recursive residual is replaced by r = b - (A^H W A + lambda) x through the same
+ * operator; p then restarts as r (direction 0, "restart") or continues as r + beta p
+ * (direction 1, "beta").  The residual history records the replaced residual.  A zero period
+ * is tsn_cg_sense. */
+typedef struct tsn_cg_options {
+  int32_t reliable_update_period;
+  int32_t reliable_update_direction;
+  int32_t reserved[6];
+} tsn_cg_options;
+tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, const float* density,
+                           float lambda, float operator_scale, int32_t iters,
+                           const tsn_cg_options* options, void* x, double* residual_history,
+                           tsn_cg_status* status, tsn_stream_t stream);
 
 /* ---- batches of independent reconstructions ------------------------------------------- */
 /* The reference runs one case per CG process (nufft_fp16x2_cg_bench.cu:279-297 argv).  A

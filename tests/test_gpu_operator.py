@@ -181,3 +181,51 @@ def test_long_cg_stays_on_the_fp64_path(iters):
     nd = onudft.Nudft(traj, n)
     x_ref, _, _ = oracle_cg(lambda v: nd.forward(v, s), lambda v: nd.adjoint(v, s), measurement(name), w, iters, 1e-4)
     assert oop.magnitude_nrmse(x_gpu.cpu().numpy(), x_ref) <= 2e-3
+
+
+def _oracle_reliable_cg(fwd, adj, y, w, iters, lam, period, direction):
+    """FP64 restatement of the reference's reliable-update CG (reference_sparse_solver.py:200-332)."""
+    wy = y if w is None else y * w[None]
+    M = lambda v: adj(fwd(v) * (1.0 if w is None else w[None])) + lam * v
+    b = adj(wy)
+    x = np.zeros_like(b)
+    r = b.copy()
+    p = r.copy()
+    rs_old = np.vdot(r, r).real
+    res = [np.sqrt(rs_old)]
+    for it in range(iters):
+        ap = M(p)
+        alpha = rs_old / np.vdot(p, ap).real
+        x = x + alpha * p
+        r = r - alpha * ap
+        rs_new = np.vdot(r, r).real
+        if period > 0 and (it + 1) % period == 0 and it + 1 < iters:
+            r = b - M(x)
+            rs_new = np.vdot(r, r).real
+            p = r.copy() if direction == "restart" else r + (rs_new / rs_old) * p
+        else:
+            p = r + (rs_new / rs_old) * p
+        res.append(np.sqrt(rs_new))
+        rs_old = rs_new
+    return x, np.array(res)
+
+
+@pytest.mark.parametrize("direction", ["restart", "beta"])
+def test_reliable_update_cg_matches_fp64(direction):
+    name = "cfg0"
+    traj, x, s, n, g, c, j, readout = case(name)
+    plan = _plan(name)
+    _, st, yt = torch_inputs(name)
+    from trajsparsenufft_b200 import synth
+    w = synth.ramp_density(traj, readout)
+    iters, period = 30, 10
+    x_gpu, hist, status = plan.cg_sense(yt, st, density=torch.from_numpy(w).cuda(), lam=1e-4, iters=iters,
+                                        reliable_update_period=period, reliable_update_direction=direction)
+    assert status["positive_curvature"] and status["finite"] and status["completed_iterations"] == iters
+    nd = onudft.Nudft(traj, n)
+    x_ref, res_ref = _oracle_reliable_cg(lambda v: nd.forward(v, s), lambda v: nd.adjoint(v, s), measurement(name),
+                                         w.astype(np.float64), iters, 1e-4, period, direction)
+    assert oop.magnitude_nrmse(x_gpu.cpu().numpy(), x_ref) <= 2e-3
+    # the replaced residuals (after iterations 10 and 20) follow the FP64 reliable residuals
+    np.testing.assert_allclose(hist[[period, 2 * period]], res_ref[[period, 2 * period]], rtol=2e-2)
+    np.testing.assert_allclose(hist[:period], res_ref[:period], rtol=2e-3)

@@ -28,7 +28,7 @@ EXPORTED = (
     "tsn_version", "tsn_get_last_error_string", "tsn_plan_desc_default", "tsn_kb_interpolation_csr",
     "tsn_kb_deapodization", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
     "tsn_plan_create_from_pack", "tsn_plan_create_from_trajectory", "tsn_plan_destroy", "tsn_plan_get_info",
-    "tsn_forward", "tsn_adjoint", "tsn_cg_sense", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
+    "tsn_forward", "tsn_adjoint", "tsn_cg_sense", "tsn_cg_sense_ex", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
     "tsn_fft_forward_panel", "tsn_fft_adjoint_image", "tsn_profile_stages", "tsn_fft_adjoint_image_static",
     "tsn_interp_component",
 )
@@ -57,6 +57,11 @@ class PlanInfo(C.Structure):
         ("nnz", C.c_int64 * 2), ("pack_bytes", C.c_int64 * 2), ("workspace_bytes", C.c_int64),
         ("plan_seconds", C.c_double), ("interp", C.c_int32), ("reserved", C.c_int32 * 7),
     ]
+
+
+class CgOptions(C.Structure):
+    _fields_ = [("reliable_update_period", C.c_int32), ("reliable_update_direction", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class CgStatus(C.Structure):
@@ -101,6 +106,8 @@ def lib() -> C.CDLL:
         "tsn_forward": (C.c_int, [P, P, P, P, P]),
         "tsn_adjoint": (C.c_int, [P, P, P, P, P]),
         "tsn_cg_sense": (C.c_int, [P, P, P, P, F32, F32, I32, P, PF64, C.POINTER(CgStatus), P]),
+        "tsn_cg_sense_ex": (C.c_int, [P, P, P, P, F32, F32, I32, C.POINTER(CgOptions), P, PF64,
+                                      C.POINTER(CgStatus), P]),
         "tsn_batch_create": (C.c_int, [C.POINTER(P), I32, I32, C.POINTER(P)]),
         "tsn_batch_destroy": (C.c_int, [P]),
         "tsn_batch_cg_sense": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), F32, F32, I32,

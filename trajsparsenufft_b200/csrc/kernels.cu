@@ -464,9 +464,9 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto issue = [&](int i0) {
     const size_t off = static_cast<size_t>(i0) * N;
-    if (mode == 1) {
+    if (mode >= 1) {
       cp_async_bytes(row0, r + off, N * 8);
-      if (iter > 0) cp_async_bytes(row1, p + off, N * 8);
+      if (mode == 1 && iter > 0) cp_async_bytes(row1, p + off, N * 8);
     } else if (f.smaps) {
       cp_async_bytes(row0, x + off, N * 8);
     }
@@ -486,7 +486,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
     if (blockIdx.x == 0 && threadIdx.x == 0) st->sigma_x = sigma;
   } else {
     sigma = pow2_scale(total, static_cast<double>(N) * N, kPanelTarget);
-    beta = iter == 0 ? 0.0 : total / fmax(st->rho[iter - 1], 1e-30);
+    beta = (iter == 0 || mode == 2) ? 0.0 : total / fmax(st->rho[iter - 1], 1e-30);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       st->rho[iter] = total;
       st->beta[iter] = beta;
@@ -505,10 +505,10 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
     }
     cp_async_wait<0>();
     __syncthreads();
-    if (mode == 1) {  // p = r + beta p (p = r at iteration 0); row0 becomes p
+    if (mode >= 1) {  // p = r + beta p (p = r at iteration 0 and after a restart); row0 becomes p
       for (int i = threadIdx.x; i < N; i += blockDim.x) {
         float2 pv = row0[i];
-        if (iter > 0) {
+        if (mode == 1 && iter > 0) {
           const float2 po = row1[i];
           pv = make_float2(pv.x + bf * po.x, pv.y + bf * po.y);
         }
@@ -527,7 +527,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
       float2 val = make_float2(0.f, 0.f);
       if (i1 < N) {
         const float d = srow[i1] * scl;
-        val = (f.smaps || mode == 1) ? cscale(cmul(row0[i1], maps[c * N + i1]), d) : cscale(maps[c * N + i1], d);
+        val = (f.smaps || mode >= 1) ? cscale(cmul(row0[i1], maps[c * N + i1]), d) : cscale(maps[c * N + i1], d);
       }
       v[j] = val;
     }
@@ -726,7 +726,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
   uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
   float2* emaps = reinterpret_cast<float2*>(reg + region);
   float2* eprow = emaps + (f.smaps ? C * N : 0);
-  float* escale = reinterpret_cast<float*>(eprow + (mode == 2 ? N : 0));
+  float* escale = reinterpret_cast<float*>(eprow + (mode >= 2 ? N : 0));
   __shared__ double red[33];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto issue = [&](int i0) {
@@ -740,7 +740,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
       const size_t off = static_cast<size_t>(i0) * N;
       if (f.smaps)
         for (int c = 0; c < C; ++c) cp_async_bytes(emaps + c * N, f.smaps + static_cast<size_t>(c) * N * N + off, N * 8);
-      if (mode == 2) cp_async_bytes(eprow, p + off, N * 8);
+      if (mode >= 2) cp_async_bytes(eprow, p + off, N * 8);
       cp_async_bytes(escale, f.scaling + off, N * 4);
     }
     cp_async_commit();
@@ -749,6 +749,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
   if (blockIdx.x < N) issue(blockIdx.x);
   float factor;
   if (mode == 2) factor = static_cast<float>(G) / st->sigma[iter] * inv_scale2;
+  else if (mode == 3) factor = static_cast<float>(G) / st->sigma_x * inv_scale2;
   else factor = inv_scale2 / st->sigma_y;
   const int c = warp;
   const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
@@ -801,8 +802,15 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
         const float2 pv = epi_smem ? eprow[i1] : p[pix];
         acc.x += lambda_scaled * pv.x;
         acc.y += lambda_scaled * pv.y;
-        out[pix] = acc;
-        dot += static_cast<double>(pv.x) * acc.x + static_cast<double>(pv.y) * acc.y;
+        if (mode == 2) {
+          out[pix] = acc;
+          dot += static_cast<double>(pv.x) * acc.x + static_cast<double>(pv.y) * acc.y;
+        } else {  // reliable residual r = b - M v (b read through x)
+          const float2 bv = x[pix];
+          const float2 rv = make_float2(bv.x - acc.x, bv.y - acc.y);
+          out[pix] = rv;
+          dot += static_cast<double>(rv.x) * rv.x + static_cast<double>(rv.y) * rv.y;
+        }
       }
     }
     if (mode != 0) {
@@ -908,7 +916,7 @@ static size_t inv_rows_region(const FftArgs& f) {
 }
 static size_t inv_rows_epi(const FftArgs& f, int mode) {
   const size_t maps = f.smaps ? sizeof(float2) * static_cast<size_t>(f.C) * f.N : 0;
-  const size_t prow = mode == 2 ? sizeof(float2) * static_cast<size_t>(f.N) : 0;
+  const size_t prow = mode >= 2 ? sizeof(float2) * static_cast<size_t>(f.N) : 0;
   return align16(maps + prow + sizeof(float) * static_cast<size_t>(f.N));
 }
 

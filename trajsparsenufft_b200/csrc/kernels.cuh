@@ -108,6 +108,7 @@ void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t
 // forward rows: x (image [N][N] with smaps, coil images [C][N][N] without) -> z1 [G][N][C]
 // mode 0: plain, sigma from norm partials -> state->sigma_x
 // mode 1: CG iteration k: p = r + beta p (p = r at k == 0), rho_k from rr partials
+// mode 2: CG iteration k after a reliable restart: p = r (beta = 0)
 void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
                      const double* partials, int nparts, CgState* st, int iter, cudaStream_t s);
 // forward columns: z1 -> panel [G*G][4C] (row q1*G + q0), FP16 hi | res
@@ -121,6 +122,8 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
 // mode 0: plain adjoint (factor 1/sigma_y): out = [N][N] (smaps) or [C][N][N]
 // mode 1: CG RHS: r = b, x = 0, rr partials
 // mode 2: CG iteration k: ap = factor*AHAp + lambda p, pap partials
+// mode 3: reliable residual: out = x - (factor*AHAp + lambda p) with x = the right-hand
+//         side b, p = the iterate and factor from the plain forward's sigma_x; rr partials
 void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r,
                      const float2* p, double* partials, CgState* st, int iter, float inv_scale2,
                      float lambda_scaled, cudaStream_t s);

@@ -88,9 +88,10 @@ struct GraphKey {
   int iters;
   uint32_t lam_bits, scale_bits;
   cudaStream_t stream;
+  int reliable;  // reliable-update period * 2 + direction
   bool operator<(const GraphKey& o) const {
-    return std::tie(y, smaps, density, x, iters, lam_bits, scale_bits, stream) <
-           std::tie(o.y, o.smaps, o.density, o.x, o.iters, o.lam_bits, o.scale_bits, o.stream);
+    return std::tie(y, smaps, density, x, iters, lam_bits, scale_bits, stream, reliable) <
+           std::tie(o.y, o.smaps, o.density, o.x, o.iters, o.lam_bits, o.scale_bits, o.stream, o.reliable);
   }
 };
 
@@ -103,7 +104,7 @@ struct tsn_plan {
   int N = 0, G = 0, C = 0, J = 0, ncomp = 0, shift = 0, rowh = 0;
   int64_t M = 0;
   DevView view[2];
-  DeviceBuffer scaling, tw, z1, panel, spanel, grid, r, p, ap, parts_pap, parts_rr, norm_parts, state;
+  DeviceBuffer scaling, tw, z1, panel, spanel, grid, r, p, ap, rhs, parts_pap, parts_rr, norm_parts, state;
   tsn_plan_info info{};
   std::map<GraphKey, cudaGraphExec_t> graphs;
   ~tsn_plan() {
@@ -283,6 +284,8 @@ void check_desc(const tsn_plan_desc* d) {
   if (d->im_size <= 0 || d->im_size % 2 || d->grid_size < d->im_size) fail(TSN_ERR_SHAPE, "need an even image size <= grid size");
   if (d->coils < 4 || d->coils > 16 || d->coils % 4) fail(TSN_ERR_UNSUPPORTED, "coil count must be 4, 8, 12 or 16");
   if (d->kernel_width < 1 || d->kernel_width > 16) fail(TSN_ERR_ARG, "kernel width out of range");
+  if (d->interp != TSN_INTERP_AUTO && d->interp != TSN_INTERP_MMA_SP)
+    fail(TSN_ERR_UNSUPPORTED, "only the mma.sp interpolation kernel is built (16-row pack tiles)");
 }
 
 // FFT endpoints are built for power-of-two grids of 128..1024 points.
@@ -318,6 +321,7 @@ void allocate_workspaces(tsn_plan* P) {
   P->r.alloc(sizeof(float2) * N * N);
   P->p.alloc(sizeof(float2) * N * N);
   P->ap.alloc(sizeof(float2) * N * N);
+  P->rhs.alloc(sizeof(float2) * N * N);
   P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(N, kNormParts));
   P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(N, kNormParts));
   P->norm_parts.alloc(sizeof(double) * kNormParts);
@@ -630,8 +634,13 @@ void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cuda
   launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, o, s);
 }
 
+// The CG-SENSE solve (launch_cg, nufft_fp16x2_cg_bench.cu:241-268). With reliable_period > 0,
+// after every reliable_period-th iteration except the last the recursive residual is replaced
+// by r = b - M x through the same operator and p restarts as r (direction 0) or continues as
+// r + beta p (direction 1), as in reference_sparse_solver.py:297-323.
 void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* density, float lambda, float scale,
-                int iters, void* x, cudaStream_t s, int share = 1) {
+                int iters, void* x, cudaStream_t s, int share = 1, int reliable_period = 0,
+                int reliable_direction = 0) {
   const FftArgs f = fft_args(P, smaps, share);
   CgState* st = P->state.as<CgState>();
   const float inv_s2 = 1.0f / (scale * scale);
@@ -642,8 +651,12 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
   enqueue_adjoint_grid(P, y, density, s, share);
   launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
   launch_inv_rows(f, P->z1.as<float2>(), nullptr, 1, X, R, nullptr, rr, st, 0, inv_s2, 0.f, s);
+  if (reliable_period > 0)  // keep b for the reliable residuals
+    CUDA_OK(cudaMemcpyAsync(P->rhs.ptr, R, P->rhs.bytes, cudaMemcpyDeviceToDevice, s));
+  bool restart = false;
   for (int k = 0; k < iters; ++k) {
-    launch_fwd_rows(f, nullptr, P->z1.as<float2>(), 1, Pv, R, rr, P->N, st, k, s);
+    launch_fwd_rows(f, nullptr, P->z1.as<float2>(), restart ? 2 : 1, Pv, R, rr, P->N, st, k, s);
+    restart = false;
     launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
     InterpOut of;
     of.panel = P->spanel.as<__half>();
@@ -659,6 +672,17 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
     launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, k, inv_s2, lam, s);
     launch_cg_update(P->N, X, R, Pv, AP, pap, rr, st, k, s);
+    if (reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters) {
+      // r = b - (A^H W A + lambda) x: plain forward of x, then the adjoint into residual mode
+      launch_norm_partials(X, static_cast<int64_t>(P->N) * P->N, P->norm_parts.as<double>(), s);
+      launch_fwd_rows(f, X, P->z1.as<float2>(), 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, s);
+      launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
+      launch_interp(interp_view(P, TSN_VIEW_G, share), P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
+      launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
+      launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
+      launch_inv_rows(f, P->z1.as<float2>(), R, 3, P->rhs.as<float2>(), nullptr, X, rr, st, k, inv_s2, lam, s);
+      restart = reliable_direction == 0;
+    }
   }
   launch_cg_finish(P->N, rr, st, iters, s);
 }
@@ -726,10 +750,13 @@ tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x
   }
 }
 
-tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const float* density, float lambda,
-                        float operator_scale, int32_t iters, void* x, double* residual_history,
-                        tsn_cg_status* status, tsn_stream_t stream) {
+tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, const float* density, float lambda,
+                           float operator_scale, int32_t iters, const tsn_cg_options* options, void* x,
+                           double* residual_history, tsn_cg_status* status, tsn_stream_t stream) {
   try {
+    const int period = options ? options->reliable_update_period : 0;
+    const int direction = options ? options->reliable_update_direction : 0;
+    if (period < 0 || direction < 0 || direction > 1) fail(TSN_ERR_ARG, "invalid reliable-update options");
     if (!plan || !y || !smaps || !x) fail(TSN_ERR_ARG, "NULL argument (y, smaps and x are required)");
     if (iters < 0 || iters > kMaxCgIter) fail(TSN_ERR_ARG, "iteration count out of range");
     if (!(operator_scale > 0.0f) || !std::isfinite(lambda)) fail(TSN_ERR_ARG, "invalid operator scale or lambda");
@@ -737,7 +764,7 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
     if (reinterpret_cast<uintptr_t>(density) & 3u) fail(TSN_ERR_ARG, "density must be 4-byte aligned");
     need_views(plan, true, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    GraphKey key{y, smaps, density, x, iters, 0, 0, s};
+    GraphKey key{y, smaps, density, x, iters, 0, 0, s, period * 2 + direction};
     std::memcpy(&key.lam_bits, &lambda, 4);
     std::memcpy(&key.scale_bits, &operator_scale, 4);
     auto it = plan->graphs.find(key);
@@ -750,7 +777,7 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
       }
       cudaGraph_t g = nullptr;
       CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
-      enqueue_cg(plan, y, smaps, density, lambda, operator_scale, iters, x, cap);
+      enqueue_cg(plan, y, smaps, density, lambda, operator_scale, iters, x, cap, 1, period, direction);
       const cudaError_t launch_err = cudaGetLastError();
       const cudaError_t end_err = cudaStreamEndCapture(cap, &g);
       if (own) cudaStreamDestroy(cap);
@@ -776,6 +803,13 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
   } catch (const std::exception& e) {
     return guard_status(e);
   }
+}
+
+tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const float* density, float lambda,
+                        float operator_scale, int32_t iters, void* x, double* residual_history,
+                        tsn_cg_status* status, tsn_stream_t stream) {
+  return tsn_cg_sense_ex(plan, y, smaps, density, lambda, operator_scale, iters, nullptr, x, residual_history, status,
+                         stream);
 }
 
 tsn_status tsn_batch_create(tsn_plan* const* plans, int32_t count, int32_t streams, tsn_batch** out) {

@@ -146,11 +146,13 @@ class Plan:
         return out
 
     def cg_sense(self, y, smaps, *, density=None, lam=1e-4, iters=10, operator_scale=1.0, out=None, stream=None,
-                 sync=True):
+                 sync=True, reliable_update_period=0, reliable_update_direction="restart"):
         """CG-SENSE solve of (A^H W A + lam) x = A^H W y from x0 = 0 (one CUDA graph).
 
         Returns (x, residual history or None, status dict or None).  With sync=False
-        the call is fully asynchronous and no host-side status is produced.
+        the call is fully asynchronous and no host-side status is produced.  A positive
+        reliable_update_period replaces the recursive residual by b - M x after every that
+        many iterations, with p restarted ("restart") or continued ("beta").
         """
         torch = _torch()
         cf = torch.complex64
@@ -163,8 +165,14 @@ class Plan:
         xp = _dev_ptr(out, cf, (n, n), "out")
         hist = np.zeros(iters + 1, dtype=np.float64) if sync else None
         st = CgStatus() if sync else None
-        rc = lib().tsn_cg_sense(self._h, yp, sp, dp, float(lam), float(operator_scale), int(iters), xp,
-                                ptr(hist, C.c_double), C.byref(st) if sync else None, _stream_handle(stream))
+        if reliable_update_direction not in ("restart", "beta"):
+            raise ValueError("reliable_update_direction must be 'restart' or 'beta'")
+        opts = _lib.CgOptions()
+        opts.reliable_update_period = int(reliable_update_period)
+        opts.reliable_update_direction = 0 if reliable_update_direction == "restart" else 1
+        rc = lib().tsn_cg_sense_ex(self._h, yp, sp, dp, float(lam), float(operator_scale), int(iters),
+                                   C.byref(opts), xp, ptr(hist, C.c_double), C.byref(st) if sync else None,
+                                   _stream_handle(stream))
         status = None
         if sync:
             status = {"completed_iterations": st.completed_iterations,
