@@ -86,7 +86,10 @@ typedef struct tsn_plan_desc {
   int32_t flags;        /* TSN_FLAG_*                                                    */
   int32_t interp;       /* TSN_INTERP_*                                                  */
   int32_t device;       /* CUDA device ordinal the plan lives on (made current at every call) */
-  int32_t reserved[6];
+  int32_t dims;         /* 2 (0 also means 2): [N][N] images; 3: [N][N][N] volumes on a G^3
+                           grid (trajectory [M][3], centred layout, fast/optimized planner,
+                           G^3 <= 2^24 cells, M <= 2^24 samples)                          */
+  int32_t reserved[5];
 } tsn_plan_desc;
 
 typedef struct tsn_plan_info {
@@ -97,7 +100,8 @@ typedef struct tsn_plan_info {
   int64_t workspace_bytes;    /* device workspace owned by the plan            */
   double plan_seconds;        /* host planner wall time                        */
   int32_t interp;             /* kernel actually used (TSN_INTERP_MMA_SP)              */
-  int32_t reserved[7];
+  int32_t dims;               /* 2 or 3                                                 */
+  int32_t reserved[6];
 } tsn_plan_info;
 
 typedef struct tsn_cg_status {
@@ -126,6 +130,15 @@ tsn_status tsn_kb_interpolation_csr(const float* traj_cycles, int64_t m, int32_t
                                     int64_t* cols, double* re, double* im, int64_t* nnz);
 /* [N][N] deapodization table (the scaling.f32.bin role, export_real_runtime_inputs.py:97-101). */
 tsn_status tsn_kb_deapodization(int32_t im_size, int32_t grid_size, int32_t width, double* out);
+
+/* Volumes: real KB weights of a [M][3] trajectory for the centred-image layout, CSR over
+ * samples, cells (q0 G + q1) G + q2, weight (phi0 phi1) phi2, columns sorted, zeros dropped
+ * (the 3D extension of tsn_kb_interpolation_csr; the reference is 2D only).  Same two-call
+ * pattern on *nnz. */
+tsn_status tsn_kb_weights_csr3(const float* traj_cycles, int64_t m, int32_t im_size, int32_t grid_size,
+                               int32_t width, int64_t* row_ptr, int64_t* cols, double* w, int64_t* nnz);
+/* [N][N][N] deapodization of the volume layout. */
+tsn_status tsn_kb_deapodization3(int32_t im_size, int32_t grid_size, int32_t width, double* out);
 
 /* Pack one view of a complex sparse matrix given as CSR over samples (G) and write the
  * production directories out_dir/real and out_dir/imag (packed_header_v2 + six arrays +
@@ -166,7 +179,10 @@ tsn_status tsn_plan_create_from_pack(const char* fwd_real_dir, const char* fwd_i
                                      const char* adj_real_dir, const char* adj_imag_dir,
                                      const float* scaling, const tsn_plan_desc* desc,
                                      tsn_plan** plan);
-/* Build both packs from a trajectory with the C++ planner (pack once) and upload them. */
+/* Build both packs from a trajectory with the C++ planner (pack once) and upload them.
+ * traj_cycles is [M][desc->dims] in cycles/pixel, [-0.5, 0.5].  Volumes (dims 3): x, smaps
+ * and coil images are [N][N][N] / [C][N][N][N], the grid has G^3 cells, and the operators,
+ * CG-SENSE, batches and stage profiling take the same calls as images. */
 tsn_status tsn_plan_create_from_trajectory(const float* traj_cycles, int64_t m,
                                            const tsn_plan_desc* desc, tsn_plan** plan);
 tsn_status tsn_plan_destroy(tsn_plan* plan);
@@ -264,7 +280,9 @@ enum {
   TSN_STAGE_INV_COLS = 4,   /* inverse FFT first stage                                       */
   TSN_STAGE_INV_ROWS = 5,   /* inverse FFT second stage + crop + deapod + coil combine      */
   TSN_STAGE_CG_UPDATE = 6,  /* x, r updates + FP64 partial dots                              */
-  TSN_STAGE_COUNT = 7
+  TSN_STAGE_FWD_MID = 7,    /* volumes: forward FFT over the middle axis (0 ms for images)   */
+  TSN_STAGE_INV_MID = 8,    /* volumes: inverse FFT over the middle axis (0 ms for images)   */
+  TSN_STAGE_COUNT = 9
 };
 /* Runs one CG-SENSE solve of `iters` iterations to populate the workspaces, then times each
  * stage of a CG iteration `reps` times in isolation with CUDA events on `stream` and writes

@@ -116,3 +116,47 @@ def to_scipy(row_ptr, cols, re, im, n_cols):
     import scipy.sparse as sp
     vals = re + 1j * im
     return sp.csr_matrix((vals, cols, row_ptr), shape=(len(row_ptr) - 1, n_cols))
+
+
+def weights_csr3(trajectory: np.ndarray, im_size: int, grid_size: int, width: int,
+                 beta: float | None = None):
+    """3D real KB weights as CSR (row_ptr, cols, w), FP64, for the centred-image layout.
+
+    The image sits centred on the grid (grid position n holds image index
+    (n + N//2) mod G), so the phase exp(2*pi*i*q.c/G) of the corner layout is
+    not needed and the coefficients are the real tensor-product weights
+    w = (phi(u0-q0) * phi(u1-q1)) * phi(u2-q2).  Rows are samples in
+    trajectory order; columns are cells (q0*G + q1)*G + q2 with q_d wrapped
+    mod G, sorted ascending; exact zeros are dropped.  The 2D rules of
+    interpolation_csr extended by one axis (the reference itself is 2D only).
+    """
+    if beta is None:
+        beta = beatty_beta(width, grid_size / im_size)
+    traj = np.asarray(trajectory, dtype=np.float64).reshape(-1, 3)
+    m = traj.shape[0]
+    u = traj * grid_size
+    start = np.floor(u - width / 2.0).astype(np.int64) + 1
+    q = start[:, :, None] + np.arange(width, dtype=np.int64)[None, None, :]   # [m, 3, J]
+    w = kb_weight(u[:, :, None] - q, width, beta)
+    wq = np.mod(q, grid_size)
+    w3 = (w[:, 0, :, None, None] * w[:, 1, None, :, None]) * w[:, 2, None, None, :]
+    cols = ((wq[:, 0, :, None, None] * grid_size + wq[:, 1, None, :, None]) * grid_size
+            + wq[:, 2, None, None, :])
+    w3 = w3.reshape(m, -1)
+    cols = cols.reshape(m, -1)
+    order = np.argsort(cols, axis=1, kind="stable")
+    cols = np.take_along_axis(cols, order, axis=1)
+    w3 = np.take_along_axis(w3, order, axis=1)
+    keep = w3 != 0.0
+    row_ptr = np.zeros(m + 1, dtype=np.int64)
+    row_ptr[1:] = np.cumsum(keep.sum(axis=1))
+    return row_ptr, cols[keep].astype(np.int64), w3[keep]
+
+
+def deapodization3(im_size: int, grid_size: int, width: int, beta: float | None = None) -> np.ndarray:
+    """[N, N, N] real deapodization (inv[a] * inv[b]) * inv[c]."""
+    if beta is None:
+        beta = beatty_beta(width, grid_size / im_size)
+    t = np.arange(im_size, dtype=np.float64) - im_size // 2
+    inv = 1.0 / kb_fourier(t / grid_size, width, beta)
+    return (inv[:, None, None] * inv[None, :, None]) * inv[None, None, :]

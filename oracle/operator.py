@@ -11,6 +11,8 @@ FP16 or the FP16 high + FP16 residual split of ``dense_components`` :66-76).
 The adjoint is the exact conjugate transpose: conjugated component products,
 unnormalized inverse FFT, crop, deapodize, coil combine with conj(S).
 
+``KbSenseOperator3`` is the same operator for volumes (real weights, centred image).
+
 ``cg_sense`` restates the CG recursion with its status dictionary
 (reference_sparse_solver.py:200-332, without the reliable-update options).
 """
@@ -128,6 +130,68 @@ class KbSenseOperator:
         grid = grid.reshape(c, self.g, self.g)
         img = scipy.fft.ifft2(grid, workers=self.workers) * float(self.g * self.g)
         return img[:, : self.n, : self.n] * self.scaling[None]
+
+    def adjoint(self, samples, smaps) -> np.ndarray:
+        coil = self.adjoint_coils(samples)
+        return np.sum(np.conj(np.asarray(smaps, dtype=np.complex128)) * coil, axis=0)
+
+
+class KbSenseOperator3:
+    """Volume SENSE NUFFT with real KB weights on the centred layout (FP64 by default).
+
+    Forward: x * S_c * deapodization placed centred on the G^3 grid (image index i at
+    grid position (i - N//2) mod G on every axis), unnormalized 3D FFT, then the real
+    weight matrix of kb.weights_csr3 (cells (q0*G + q1)*G + q2).  Adjoint: the exact
+    conjugate transpose.  matrix_mode / panel_mode emulate the FP16 weights and the
+    FP16 high + residual panels as KbSenseOperator does for images.
+    """
+
+    def __init__(self, trajectory, im_size: int, grid_size: int, width: int,
+                 matrix_mode: str = "fp64", panel_mode: str = "fp64", workers: int = 1):
+        self.n = im_size
+        self.g = grid_size
+        self.workers = workers
+        self.panel_mode = panel_mode
+        row_ptr, cols, w = kb.weights_csr3(trajectory, im_size, grid_size, width)
+        w = _quantize_matrix(w, matrix_mode)
+        self.m = len(row_ptr) - 1
+        self.w = sp.csr_matrix((w, cols, row_ptr), shape=(self.m, grid_size ** 3))
+        self.wt = self.w.T.tocsr()
+        self.scaling = kb.deapodization3(im_size, grid_size, width)
+        self._pos = (np.arange(im_size) - im_size // 2) % grid_size
+
+    def grid_panel(self, image, smaps) -> np.ndarray:
+        """[G^3, C] complex panel = FFT3(centred pad(x * S_c * scaling))."""
+        coil = np.asarray(image, dtype=np.complex128)[None] * np.asarray(smaps, dtype=np.complex128)
+        return self.grid_panel_coils(coil)
+
+    def grid_panel_coils(self, coil) -> np.ndarray:
+        coil = np.asarray(coil, dtype=np.complex128) * self.scaling[None]
+        c, g, pos = coil.shape[0], self.g, self._pos
+        grid = np.zeros((c, g, g, g), dtype=np.complex128)
+        grid[np.ix_(np.arange(c), pos, pos, pos)] = coil
+        z = scipy.fft.fftn(grid, axes=(1, 2, 3), workers=self.workers)
+        return z.reshape(c, -1).T
+
+    def interp(self, panel: np.ndarray) -> np.ndarray:
+        pr = dense_components(panel.real, self.panel_mode)
+        pi = dense_components(panel.imag, self.panel_mode)
+        return (self.w @ pr + 1j * (self.w @ pi)).T
+
+    def interp_adjoint(self, samples: np.ndarray) -> np.ndarray:
+        panel = np.asarray(samples).T
+        pr = dense_components(panel.real, self.panel_mode)
+        pi = dense_components(panel.imag, self.panel_mode)
+        return (self.wt @ pr + 1j * (self.wt @ pi)).T
+
+    def forward(self, image, smaps) -> np.ndarray:
+        return self.interp(self.grid_panel(image, smaps))
+
+    def adjoint_coils(self, samples) -> np.ndarray:
+        grid = self.interp_adjoint(samples)
+        c, g, pos = grid.shape[0], self.g, self._pos
+        vol = scipy.fft.ifftn(grid.reshape(c, g, g, g), axes=(1, 2, 3), workers=self.workers) * float(g ** 3)
+        return vol[np.ix_(np.arange(c), pos, pos, pos)] * self.scaling[None]
 
     def adjoint(self, samples, smaps) -> np.ndarray:
         coil = self.adjoint_coils(samples)

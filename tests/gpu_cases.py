@@ -69,3 +69,27 @@ def torch_inputs(name: str, dev="cuda"):
     y = measurement(name)
     return (torch.from_numpy(np.ascontiguousarray(x)).to(dev), torch.from_numpy(np.ascontiguousarray(s)).to(dev),
             torch.from_numpy(np.ascontiguousarray(y)).to(dev))
+
+
+@functools.lru_cache(maxsize=None)
+def volume_case(name: str):
+    """(trajectory [M,3], volume, smaps, N, G, C, J) of a named 3D kooshball configuration."""
+    if name == "vol64":           # 64^3 on a 128^3 grid, 4 coils, 512 x 128 golden-means kooshball
+        n, g, c, spokes, readout = 64, 128, 4, 512, 128
+    elif name == "vol64c8":       # 8 coils, sparser
+        n, g, c, spokes, readout = 64, 128, 8, 256, 128
+    else:
+        raise KeyError(name)
+    traj = synth.kooshball(spokes, readout)
+    x = synth.ellipsoid_phantom(n, SEED)
+    s = synth.coil_maps3(n, c, SEED)
+    return traj, x, s, n, g, c, 4
+
+
+@functools.lru_cache(maxsize=None)
+def volume_measurement(name: str):
+    """k-space of a volume case from the FP64 KB operator with J = 6 (within ~1e-5 of the direct
+    NUDFT; the NUDFT itself is checked on a subsample) plus 1e-3 rms complex noise."""
+    traj, x, s, n, g, c, _ = volume_case(name)
+    y = oop.KbSenseOperator3(traj, n, g, 6, workers=8).forward(x, s)
+    return synth.add_noise(y, SEED)

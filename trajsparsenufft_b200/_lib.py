@@ -22,11 +22,12 @@ POLICY = {"trajectory": 0, "morton": 1, "overlap": 2, "packing256": 3}
 ILLEGAL = {"split24": 0, "csr_residual": 1}
 VIEW = {"G": 0, "G_T": 1}
 FLAG_REFERENCE_LAYOUT = 1
-STAGES = ("fwd_rows", "fwd_cols", "interp_fwd", "interp_adj", "inv_cols", "inv_rows", "cg_update")
+STAGES = ("fwd_rows", "fwd_cols", "interp_fwd", "interp_adj", "inv_cols", "inv_rows", "cg_update", "fwd_mid",
+          "inv_mid")
 
 EXPORTED = (
     "tsn_version", "tsn_get_last_error_string", "tsn_plan_desc_default", "tsn_kb_interpolation_csr",
-    "tsn_kb_deapodization", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
+    "tsn_kb_deapodization", "tsn_kb_weights_csr3", "tsn_kb_deapodization3", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
     "tsn_plan_create_from_pack", "tsn_plan_create_from_trajectory", "tsn_plan_destroy", "tsn_plan_get_info",
     "tsn_forward", "tsn_adjoint", "tsn_cg_sense", "tsn_cg_sense_ex", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
     "tsn_fft_forward_panel", "tsn_fft_adjoint_image", "tsn_profile_stages", "tsn_fft_adjoint_image_static",
@@ -45,7 +46,8 @@ class PlanDesc(C.Structure):
     _fields_ = [
         ("im_size", C.c_int32), ("grid_size", C.c_int32), ("coils", C.c_int32), ("kernel_width", C.c_int32),
         ("planner", C.c_int32), ("policy", C.c_int32), ("seed", C.c_uint64), ("threads", C.c_int32),
-        ("flags", C.c_int32), ("interp", C.c_int32), ("device", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("flags", C.c_int32), ("interp", C.c_int32), ("device", C.c_int32), ("dims", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -55,7 +57,7 @@ class PlanInfo(C.Structure):
         ("kernel_width", C.c_int32), ("components", C.c_int32),
         ("groups", C.c_int64 * 2), ("tiles", C.c_int64 * 2), ("active_rows", C.c_int64 * 2),
         ("nnz", C.c_int64 * 2), ("pack_bytes", C.c_int64 * 2), ("workspace_bytes", C.c_int64),
-        ("plan_seconds", C.c_double), ("interp", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("plan_seconds", C.c_double), ("interp", C.c_int32), ("dims", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -92,6 +94,8 @@ def lib() -> C.CDLL:
         "tsn_plan_desc_default": (C.c_int, [C.POINTER(PlanDesc)]),
         "tsn_kb_interpolation_csr": (C.c_int, [PF32, I64, I32, I32, I32, PI64, PI64, PF64, PF64, PI64]),
         "tsn_kb_deapodization": (C.c_int, [I32, I32, I32, PF64]),
+        "tsn_kb_weights_csr3": (C.c_int, [PF32, I64, I32, I32, I32, PI64, PI64, PF64, PI64]),
+        "tsn_kb_deapodization3": (C.c_int, [I32, I32, I32, PF64]),
         "tsn_pack_csr_to_dirs": (C.c_int, [PI64, PI64, PF64, PF64, I64, I32, PF32, I32, I32, I32, U64, I32,
                                            C.c_char_p]),
         "tsn_pack_view_tiles": (C.c_int, [PI64, PI64, PF64, PI64, PF64, I64, I64, I64, I32, I32, I32, U64, I32,

@@ -162,6 +162,37 @@ tsn_status tsn_kb_interpolation_csr(const float* traj, int64_t m, int32_t im_siz
   }
 }
 
+tsn_status tsn_kb_weights_csr3(const float* traj, int64_t m, int32_t im_size, int32_t grid_size, int32_t width,
+                               int64_t* row_ptr, int64_t* cols, double* w, int64_t* nnz) {
+  try {
+    if (!traj || !nnz) fail(TSN_ERR_ARG, "NULL argument");
+    const KbCsr kb = kb_weights_csr3(traj, m, im_size, grid_size, width, 0);
+    const int64_t n = static_cast<int64_t>(kb.cols.size());
+    if (cols) {
+      if (*nnz < n) fail(TSN_ERR_ARG, "output arrays too small");
+      if (!row_ptr || !w) fail(TSN_ERR_ARG, "NULL output array");
+      std::memcpy(row_ptr, kb.row_ptr.data(), sizeof(int64_t) * kb.row_ptr.size());
+      std::memcpy(cols, kb.cols.data(), sizeof(int64_t) * n);
+      std::memcpy(w, kb.re.data(), sizeof(double) * n);
+    }
+    *nnz = n;
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_kb_deapodization3(int32_t im_size, int32_t grid_size, int32_t width, double* out) {
+  try {
+    if (!out || im_size <= 0 || grid_size < im_size || width <= 0) fail(TSN_ERR_ARG, "invalid argument");
+    const auto d = deapodization3(im_size, grid_size, width);
+    std::memcpy(out, d.data(), sizeof(double) * d.size());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
 tsn_status tsn_kb_deapodization(int32_t im_size, int32_t grid_size, int32_t width, double* out) {
   try {
     if (!out || im_size <= 0 || grid_size < im_size || width <= 0) fail(TSN_ERR_ARG, "invalid argument");

@@ -10,8 +10,10 @@
 //   phase    exp(2*pi*i*q*c/G), c = N/2: the image sits at [0,N) of the padded grid
 //   deapod   1/(Phi(t0/G) Phi(t1/G)), Phi(xi) = J*sinh(z)/z/I0(beta), z^2 = beta^2-(pi*J*xi)^2
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "kb.hpp"
@@ -127,6 +129,112 @@ KbCsr kb_interpolation_csr(const float* traj, int64_t m, int im_size, int grid_s
     }
     out.row_ptr[r + 1] = static_cast<int64_t>(out.cols.size());
   }
+  return out;
+}
+
+
+std::vector<double> deapodization3(int im_size, int grid_size, int width) {
+  const double beta = beatty_beta(width, static_cast<double>(grid_size) / im_size);
+  const double i0b = bessel_i0(beta);
+  std::vector<double> inv(im_size);
+  for (int i = 0; i < im_size; ++i)
+    inv[i] = 1.0 / kb_fourier(static_cast<double>(i - im_size / 2) / grid_size, width, beta, i0b);
+  const size_t n = static_cast<size_t>(im_size);
+  std::vector<double> out(n * n * n);
+  for (size_t a = 0; a < n; ++a)
+    for (size_t b = 0; b < n; ++b)
+      for (size_t c = 0; c < n; ++c) out[(a * n + b) * n + c] = (inv[a] * inv[b]) * inv[c];
+  return out;
+}
+
+namespace {
+
+// Support start, weights and wrapped cell index of one sample along one axis.
+struct Axis {
+  int64_t cell[16];
+  double w[16];
+};
+
+inline void axis_weights(double u, int width, int64_t g, double beta, double i0b, Axis& a) {
+  const int64_t s = static_cast<int64_t>(std::floor(u - width / 2.0)) + 1;
+  for (int j = 0; j < width; ++j) {
+    const int64_t q = s + j;
+    a.w[j] = kb_weight(u - static_cast<double>(q), width, beta, i0b);
+    a.cell[j] = ((q % g) + g) % g;
+  }
+}
+
+template <class F>
+void parallel_rows(int64_t n, int threads, F&& body) {
+  threads = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(threads, n / 4096 + 1)));
+  std::atomic<int64_t> next{0};
+  auto work = [&]() {
+    for (;;) {
+      const int64_t lo = next.fetch_add(4096);
+      if (lo >= n) break;
+      const int64_t hi = std::min(n, lo + 4096);
+      for (int64_t r = lo; r < hi; ++r) body(r);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+KbCsr kb_weights_csr3(const float* traj, int64_t m, int im_size, int grid_size, int width, int threads) {
+  if (m < 0 || im_size <= 0 || grid_size < im_size || width <= 0 || width > 16 || width > grid_size)
+    fail(TSN_ERR_ARG, "invalid 3D KB interpolation shape");
+  const double beta = beatty_beta(width, static_cast<double>(grid_size) / im_size);
+  const double i0b = bessel_i0(beta);
+  const int64_t g = grid_size;
+  for (int64_t i = 0; i < 3 * m; ++i)
+    if (!std::isfinite(traj[i])) fail(TSN_ERR_NONFINITE, "trajectory contains non-finite coordinates");
+  if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+  KbCsr out;
+  out.row_ptr.assign(static_cast<size_t>(m) + 1, 0);
+  auto axes = [&](int64_t r, Axis (&ax)[3]) {
+    for (int d = 0; d < 3; ++d) axis_weights(static_cast<double>(traj[3 * r + d]) * grid_size, width, g, beta, i0b, ax[d]);
+  };
+  // pass 1: nonzero count per row
+  parallel_rows(m, threads, [&](int64_t r) {
+    Axis ax[3];
+    axes(r, ax);
+    int64_t n[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d)
+      for (int j = 0; j < width; ++j) n[d] += ax[d].w[j] != 0.0;
+    out.row_ptr[r + 1] = n[0] * n[1] * n[2];
+  });
+  for (int64_t r = 0; r < m; ++r) out.row_ptr[r + 1] += out.row_ptr[r];
+  out.cols.resize(static_cast<size_t>(out.row_ptr[m]));
+  out.re.resize(out.cols.size());
+  // pass 2: entries, sorted by cell
+  parallel_rows(m, threads, [&](int64_t r) {
+    Axis ax[3];
+    axes(r, ax);
+    std::vector<std::pair<int64_t, double>> e;
+    e.reserve(static_cast<size_t>(width) * width * width);
+    for (int a = 0; a < width; ++a) {
+      if (ax[0].w[a] == 0.0) continue;
+      for (int b = 0; b < width; ++b) {
+        if (ax[1].w[b] == 0.0) continue;
+        const double wab = ax[0].w[a] * ax[1].w[b];
+        for (int c = 0; c < width; ++c) {
+          if (ax[2].w[c] == 0.0) continue;
+          e.emplace_back((ax[0].cell[a] * g + ax[1].cell[b]) * g + ax[2].cell[c], wab * ax[2].w[c]);
+        }
+      }
+    }
+    std::sort(e.begin(), e.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    int64_t at = out.row_ptr[r];
+    for (const auto& kv : e) {
+      out.cols[at] = kv.first;
+      out.re[at] = kv.second;
+      ++at;
+    }
+  });
   return out;
 }
 

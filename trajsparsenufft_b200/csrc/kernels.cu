@@ -51,14 +51,15 @@ __device__ __forceinline__ int chunk_swizzle(int ch, int row) {
 
 constexpr int kInterpWarps = 4;
 
-// Output row s (0..15) of a record: 24-bit little-endian fields, 0xFFFFFF = pad (-1).
-__device__ __forceinline__ int32_t record_row(const uint8_t* rows24, int s) {
+// Output row s (0..15) of a record: 24-bit little-endian fields; -1 for a pad row (live bit
+// 16 + s of the record flags clear), so every one of the 2^24 row indices is addressable.
+__device__ __forceinline__ int32_t record_row(const uint8_t* rows24, int32_t flags, int s) {
   const uint32_t* w = reinterpret_cast<const uint32_t*>(rows24);
   const int bit = 24 * s, off = bit & 31;
   const uint32_t lo = w[bit >> 5];
   const uint32_t hi = off > 8 ? w[(bit >> 5) + 1] : 0u;  // stays inside the 48-byte field
   const uint32_t v = __funnelshift_r(lo, hi, off) & 0xFFFFFFu;
-  return v == static_cast<uint32_t>(kRecRowPad) ? -1 : static_cast<int32_t>(v);
+  return ((static_cast<uint32_t>(flags) >> (kRecLiveShift + s)) & 1u) ? static_cast<int32_t>(v) : -1;
 }
 
 // Per-warp shared-memory ring: stage = tile record (cols, A, meta) + 32 gathered panel rows.
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
     const uint8_t* trow = st + INFO + 16;
     if constexpr (EPI == EPI_PANEL) {  // density weights at the item's first tile
       if (o.density && (info.flags & kRecFirst)) {
-        const int32_t r0 = record_row(trow, g), r1 = record_row(trow, g + 8);
+        const int32_t r0 = record_row(trow, info.flags, g), r1 = record_row(trow, info.flags, g + 8);
         wrow[0] = r0 >= 0 ? __ldg(o.density + r0) : 1.f;
         wrow[1] = r1 >= 0 ? __ldg(o.density + r1) : 1.f;
       }
@@ -267,8 +268,8 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
     }
     int32_t rows[2] = {-1, -1};
     if (info.flags & kRecLast) {
-      rows[0] = record_row(trow, g);
-      rows[1] = record_row(trow, g + 8);
+      rows[0] = record_row(trow, info.flags, g);
+      rows[1] = record_row(trow, info.flags, g + 8);
     }
     __syncwarp();  // this stage is refilled by the next iteration's record copy
     if (info.flags & kRecLast) {  // last tile of its item
@@ -450,6 +451,8 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N;
+  const int lines = f.lines();
+  const int64_t pix = f.pix();
   constexpr int C = CC;  // coils (one warp each), a compile-time stride
   const int in_f2 = (2 + C) * N;  // float2 of the slab before the scaling row
   float2* tw_s = reinterpret_cast<float2*>(sm);
@@ -471,21 +474,21 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
       cp_async_bytes(row0, x + off, N * 8);
     }
     const float2* msrc = f.smaps ? f.smaps : x;
-    for (int c = 0; c < C; ++c) cp_async_bytes(maps + c * N, msrc + static_cast<size_t>(c) * N * N + off, N * 8);
+    for (int c = 0; c < C; ++c) cp_async_bytes(maps + c * N, msrc + static_cast<size_t>(c) * pix + off, N * 8);
     cp_async_bytes(reg + in_f2 * 8, f.scaling + off, N * 4);
     cp_async_commit();
   };
   // the first item (and the twiddles) stream in while the panel scale is reduced
   cp_async_bytes(tw_s, f.tw, G * 8);
-  if (blockIdx.x < N) issue(blockIdx.x);
+  if (blockIdx.x < lines) issue(blockIdx.x);
   const double total = sum_partials(parts, nparts, red);
   float sigma;
   double beta = 0.0;
   if (mode == 0) {
-    sigma = pow2_scale(total, static_cast<double>(N) * N * (f.smaps ? 1 : C), kPanelTarget);
+    sigma = pow2_scale(total, static_cast<double>(pix) * (f.smaps ? 1 : C), kPanelTarget);
     if (blockIdx.x == 0 && threadIdx.x == 0) st->sigma_x = sigma;
   } else {
-    sigma = pow2_scale(total, static_cast<double>(N) * N, kPanelTarget);
+    sigma = pow2_scale(total, static_cast<double>(pix), kPanelTarget);
     beta = (iter == 0 || mode == 2) ? 0.0 : total / fmax(st->rho[iter - 1], 1e-30);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       st->rho[iter] = total;
@@ -494,11 +497,11 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
     }
   }
   const float bf = static_cast<float>(beta);
-  const float scl = sigma / static_cast<float>(G);
+  const float scl = sigma / f.gs();
   // output copy: C/2 16-byte chunks per grid row, 64 rows per pass of the 32*C threads
   const int ch2 = C >> 1;
   const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
-  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x) {
+  for (int i0 = blockIdx.x; i0 < lines; i0 += gridDim.x) {
     if (i0 != blockIdx.x) {
       __syncthreads();  // the previous item's output rows are copied out
       issue(i0);
@@ -537,9 +540,11 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
 #pragma unroll
     for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * (C + 1) + c] = v[m];
     __syncthreads();
+    // line i0 = (slab, row): z1 [slab][q][row][c] (one slab for images)
+    const size_t obase = static_cast<size_t>(i0 / N) * G * N + i0 % N;
     for (int q1 = crow; q1 < G; q1 += 64) {
       const float2 a = out_s[q1 * (C + 1) + 2 * ck], b = out_s[q1 * (C + 1) + 2 * ck + 1];
-      *reinterpret_cast<float4*>(z1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * ck) = make_float4(a.x, a.y, b.x, b.y);
+      *reinterpret_cast<float4*>(z1 + (obase + static_cast<size_t>(q1) * N) * C + 2 * ck) = make_float4(a.x, a.y, b.x, b.y);
     }
   }
 }
@@ -563,14 +568,15 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_cols_kernel(FftArgs f,
     cp_async_slab(reinterpret_cast<float2*>(regs + b * region), z1 + static_cast<size_t>(q1) * N * C, N, C);
     cp_async_commit();
   };
+  const int items = f.gcols();
   cp_async_bytes(tw_s, f.tw, G * 8);
-  if (blockIdx.x < G) issue(blockIdx.x, 0);
+  if (blockIdx.x < items) issue(blockIdx.x, 0);
   const int ch2 = C >> 1;  // 16-byte chunks per panel row
   const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
   const int c = warp;
   const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane + f.shift, C >> 1)) + (c & 1);
   int it = 0;
-  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, ++it) {
+  for (int q1 = blockIdx.x; q1 < items; q1 += gridDim.x, ++it) {
     const int b = nbuf == 2 ? (it & 1) : 0;
     if (nbuf == 1 && it > 0) {
       __syncthreads();  // the previous item's output rows are copied out
@@ -578,7 +584,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_cols_kernel(FftArgs f,
     }
     cp_async_wait<0>();
     __syncthreads();
-    if (nbuf == 2 && q1 + gridDim.x < G) issue(q1 + gridDim.x, b ^ 1);
+    if (nbuf == 2 && q1 + gridDim.x < items) issue(q1 + gridDim.x, b ^ 1);
     uint8_t* reg = regs + b * region;
     const float2* in_s = reinterpret_cast<const float2*>(reg);
     float2 v[P];
@@ -608,6 +614,69 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_cols_kernel(FftArgs f,
     for (int q0 = crow; q0 < G; q0 += 64) {
       const uint32_t* s = out_s + q0 * OP + 4 * ck;
       *reinterpret_cast<uint4*>(dst + q0 * 2 * C + 4 * ck) = make_uint4(s[0], s[1], s[2], s[3]);
+    }
+  }
+}
+
+// Forward middle axis of a volume: z1[i0][q2][i1][c] -> z2[q2][q1][i0][c]. One item per
+// (i0, q2) line: its [N][C] run of z1 is contiguous; FFT over i1 with the zero padding and
+// centring shift of the other axes; each q1 writes one 8C-byte run of z2.
+// Shared memory: twiddles [G] | nbuf regions, each holding in turn the swizzled slab [N][C],
+// the per-warp FFT scratch and the output rows [G][C+1] float2.
+template <int G, int CC>
+__global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_mid_kernel(FftArgs f, const float2* __restrict__ z1,
+                                                    float2* __restrict__ z2, int region, int nbuf) {
+  constexpr int P = G / 32;
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int N = f.N;
+  constexpr int C = CC;
+  const int items = N * G;
+  float2* tw_s = reinterpret_cast<float2*>(sm);
+  uint8_t* regs = reinterpret_cast<uint8_t*>(tw_s + G);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto issue = [&](int t, int b) {
+    cp_async_slab(reinterpret_cast<float2*>(regs + b * region), z1 + static_cast<size_t>(t) * N * C, N, C);
+    cp_async_commit();
+  };
+  cp_async_bytes(tw_s, f.tw, G * 8);
+  if (blockIdx.x < items) issue(blockIdx.x, 0);
+  const int ch2 = C >> 1;
+  const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
+  const int c = warp;
+  const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane + f.shift, C >> 1)) + (c & 1);
+  int it = 0;
+  for (int t = blockIdx.x; t < items; t += gridDim.x, ++it) {
+    const int b = nbuf == 2 ? (it & 1) : 0;
+    if (nbuf == 1 && it > 0) {
+      __syncthreads();  // the previous item's output rows are copied out
+      issue(t, 0);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (nbuf == 2 && t + gridDim.x < items) issue(t + gridDim.x, b ^ 1);
+    uint8_t* reg = regs + b * region;
+    const float2* in_s = reinterpret_cast<const float2*>(reg);
+    float2 v[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const int n = warp_fft_in_index<G>(j);
+      int i1 = n + f.shift;
+      if (i1 >= G) i1 -= G;
+      const int idx = FftPlan<G>::R == 1 ? i1 * C + lane_off : slab_idx(i1, c, C);
+      v[j] = i1 < N ? in_s[idx] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();  // slab consumed
+    warp_fft<G, false>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();  // scratch free
+    float2* out_s = reinterpret_cast<float2*>(reg);  // [G][C+1]
+#pragma unroll
+    for (int m = 0; m < P; ++m) out_s[warp_fft_out_index<G>(m) * (C + 1) + c] = v[m];
+    __syncthreads();
+    const int i0 = t / G, q2 = t - (t / G) * G;
+    float2* dst = z2 + (static_cast<size_t>(q2) * G * N + i0) * C;
+    for (int q1 = crow; q1 < G; q1 += 64) {
+      const float2 a = out_s[q1 * (C + 1) + 2 * ck], bb = out_s[q1 * (C + 1) + 2 * ck + 1];
+      *reinterpret_cast<float4*>(dst + static_cast<size_t>(q1) * N * C + 2 * ck) = make_float4(a.x, a.y, bb.x, bb.y);
     }
   }
 }
@@ -662,14 +731,15 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_cols_kernel(FftArgs f,
     cp_async_slab(reinterpret_cast<float2*>(regs + b * region), grid + static_cast<size_t>(q1) * G * C, G, C);
     cp_async_commit();
   };
+  const int items = f.gcols();
   cp_async_bytes(tw_s, f.tw, G * 8);
-  if (blockIdx.x < G) issue(blockIdx.x, 0);
+  if (blockIdx.x < items) issue(blockIdx.x, 0);
   const int ch2 = C >> 1;  // 16-byte chunks per output row
   const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
   const int c = warp;
   const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
   int it = 0;
-  for (int q1 = blockIdx.x; q1 < G; q1 += gridDim.x, ++it) {
+  for (int q1 = blockIdx.x; q1 < items; q1 += gridDim.x, ++it) {
     const int b = nbuf == 2 ? (it & 1) : 0;
     if (nbuf == 1 && it > 0) {
       __syncthreads();
@@ -677,7 +747,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_cols_kernel(FftArgs f,
     }
     cp_async_wait<0>();
     __syncthreads();
-    if (nbuf == 2 && q1 + gridDim.x < G) issue(q1 + gridDim.x, b ^ 1);
+    if (nbuf == 2 && q1 + gridDim.x < items) issue(q1 + gridDim.x, b ^ 1);
     uint8_t* reg = regs + b * region;
     const float2* in_s = reinterpret_cast<const float2*>(reg);
     float2 v[P];
@@ -705,6 +775,75 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_cols_kernel(FftArgs f,
   }
 }
 
+// Inverse middle axis of a volume: z2[q2][q1][i0][c] -> z1[q2][i0][i1][c], i1 < N (crop).
+// One item per (q2, i0): G runs of C values, N*C apart, gathered into a swizzled slab; the
+// cropped output of the item is one contiguous [N][C] run.
+// Shared memory: twiddles [G] | nbuf regions, each holding in turn the slab [G][C], the
+// per-warp FFT scratch and the output rows [N][C+1] float2.
+template <int G, int CC>
+__global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_mid_kernel(FftArgs f, const float2* __restrict__ z2,
+                                                    float2* __restrict__ z1, int region, int nbuf) {
+  constexpr int P = G / 32;
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int N = f.N;
+  constexpr int C = CC;
+  const int items = G * N;
+  float2* tw_s = reinterpret_cast<float2*>(sm);
+  uint8_t* regs = reinterpret_cast<uint8_t*>(tw_s + G);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto issue = [&](int t, int b) {
+    float2* dst = reinterpret_cast<float2*>(regs + b * region);
+    const int q2 = t / N, i0 = t - (t / N) * N;
+    const float2* src = z2 + (static_cast<size_t>(q2) * G * N + i0) * C;
+    const int chn = C / 2;
+    const int k = threadIdx.x % chn;  // 32*C threads: 64 rows per pass
+    for (int q1 = threadIdx.x / chn; q1 < G; q1 += 64)
+      cp_async16(dst + q1 * C + 2 * (k ^ slab_swz(q1, chn)), src + static_cast<size_t>(q1) * N * C + 2 * k);
+    cp_async_commit();
+  };
+  cp_async_bytes(tw_s, f.tw, G * 8);
+  if (blockIdx.x < items) issue(blockIdx.x, 0);
+  const int ch2 = C >> 1;
+  const int ck = threadIdx.x % ch2, crow = threadIdx.x / ch2;
+  const int c = warp;
+  const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
+  int it = 0;
+  for (int t = blockIdx.x; t < items; t += gridDim.x, ++it) {
+    const int b = nbuf == 2 ? (it & 1) : 0;
+    if (nbuf == 1 && it > 0) {
+      __syncthreads();
+      issue(t, 0);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (nbuf == 2 && t + gridDim.x < items) issue(t + gridDim.x, b ^ 1);
+    uint8_t* reg = regs + b * region;
+    const float2* in_s = reinterpret_cast<const float2*>(reg);
+    float2 v[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const int n = warp_fft_in_index<G>(j);
+      v[j] = in_s[FftPlan<G>::R == 1 ? n * C + lane_off : slab_idx(n, c, C)];
+    }
+    __syncthreads();
+    warp_fft<G, true>(v, reinterpret_cast<float2*>(reg) + c * FftSmem<G>::SCR, tw_s);
+    __syncthreads();
+    float2* out_s = reinterpret_cast<float2*>(reg);  // [N][C+1]
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+      int i1 = warp_fft_out_index<G>(m) + f.shift;
+      if (i1 >= G) i1 -= G;
+      if (i1 < N) out_s[i1 * (C + 1) + c] = v[m];
+    }
+    __syncthreads();
+    float2* dst = z1 + static_cast<size_t>(t) * N * C;
+    for (int i1 = crow; i1 < N; i1 += 64) {
+      const float2 a = out_s[i1 * (C + 1) + 2 * ck], bb = out_s[i1 * (C + 1) + 2 * ck + 1];
+      *reinterpret_cast<float4*>(dst + i1 * C + 2 * ck) = make_float4(a.x, a.y, bb.x, bb.y);
+    }
+  }
+}
+
 // Inverse rows + crop + deapodization + SENSE coil combine (+ CG epilogues).
 // Shared memory: twiddles [G] | a region holding in turn the swizzled slab [G][C], the
 // per-warp FFT scratch and the coil images [C][N] | (epi_smem) the epilogue inputs of the
@@ -722,6 +861,8 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N;
   constexpr int C = CC;  // coils (one warp each), a compile-time stride
+  const int lines = f.lines();
+  const int64_t pix_n = f.pix();
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
   float2* emaps = reinterpret_cast<float2*>(reg + region);
@@ -735,25 +876,25 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
     const int chn = C / 2;
     const int k = threadIdx.x % chn;  // 32*C threads: 64 rows per pass
     for (int q1 = threadIdx.x / chn; q1 < G; q1 += 64)
-      cp_async16(dst + q1 * C + 2 * (k ^ slab_swz(q1, chn)), w1 + (static_cast<size_t>(q1) * N + i0) * C + 2 * k);
+      cp_async16(dst + q1 * C + 2 * (k ^ slab_swz(q1, chn)), w1 + (static_cast<size_t>(q1) * lines + i0) * C + 2 * k);
     if (epi_smem) {
       const size_t off = static_cast<size_t>(i0) * N;
       if (f.smaps)
-        for (int c = 0; c < C; ++c) cp_async_bytes(emaps + c * N, f.smaps + static_cast<size_t>(c) * N * N + off, N * 8);
+        for (int c = 0; c < C; ++c) cp_async_bytes(emaps + c * N, f.smaps + static_cast<size_t>(c) * pix_n + off, N * 8);
       if (mode >= 2) cp_async_bytes(eprow, p + off, N * 8);
       cp_async_bytes(escale, f.scaling + off, N * 4);
     }
     cp_async_commit();
   };
   cp_async_bytes(tw_s, f.tw, G * 8);
-  if (blockIdx.x < N) issue(blockIdx.x);
+  if (blockIdx.x < lines) issue(blockIdx.x);
   float factor;
-  if (mode == 2) factor = static_cast<float>(G) / st->sigma[iter] * inv_scale2;
-  else if (mode == 3) factor = static_cast<float>(G) / st->sigma_x * inv_scale2;
+  if (mode == 2) factor = f.gs() / st->sigma[iter] * inv_scale2;
+  else if (mode == 3) factor = f.gs() / st->sigma_x * inv_scale2;
   else factor = inv_scale2 / st->sigma_y;
   const int c = warp;
   const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
-  for (int i0 = blockIdx.x; i0 < N; i0 += gridDim.x) {
+  for (int i0 = blockIdx.x; i0 < lines; i0 += gridDim.x) {
     if (i0 != blockIdx.x) {
       __syncthreads();
       issue(i0);
@@ -783,12 +924,12 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
       const size_t pix = static_cast<size_t>(i0) * N + i1;
       const float d = (epi_smem ? escale[i1] : f.scaling[pix]) * factor;
       if (!f.smaps) {  // coil images out [C][N][N]
-        for (int cc = 0; cc < C; ++cc) out[static_cast<size_t>(cc) * N * N + pix] = cscale(img_s[cc * N + i1], d);
+        for (int cc = 0; cc < C; ++cc) out[static_cast<size_t>(cc) * pix_n + pix] = cscale(img_s[cc * N + i1], d);
         continue;
       }
       float2 acc = make_float2(0.f, 0.f);
       for (int cc = 0; cc < C; ++cc) {
-        const float2 s = epi_smem ? emaps[cc * N + i1] : f.smaps[static_cast<size_t>(cc) * N * N + pix];
+        const float2 s = epi_smem ? emaps[cc * N + i1] : f.smaps[static_cast<size_t>(cc) * pix_n + pix];
         acc = cadd(acc, cmulc(img_s[cc * N + i1], s));
       }
       acc = cscale(acc, d);
@@ -822,9 +963,10 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
 
 constexpr int kCgRowPix = 4;  // pixels per thread of cg_update: rows up to 1024 pixels at 256 threads
 
-__global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
-                                 const float2* __restrict__ ap, const double* __restrict__ pap_parts,
-                                 double* __restrict__ rr_parts, CgState* __restrict__ st, int iter) {
+__global__ void cg_update_kernel(int N, int nparts, float2* __restrict__ x, float2* __restrict__ r,
+                                 const float2* __restrict__ p, const float2* __restrict__ ap,
+                                 const double* __restrict__ pap_parts, double* __restrict__ rr_parts,
+                                 CgState* __restrict__ st, int iter) {
   __shared__ double red[33];
   // the row's vectors stream in while the pAp partials are reduced (N <= kCgRowPix * blockDim)
   const int i0 = blockIdx.x;
@@ -840,7 +982,7 @@ __global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restri
       rv[j] = r[pix];
     }
   }
-  const double pap = sum_partials(pap_parts, N, red);
+  const double pap = sum_partials(pap_parts, nparts, red);
   const double rho = st->rho[iter];
   const bool ok = isfinite(pap) && pap > 0.0;
   const double alpha = ok ? rho / pap : 0.0;
@@ -870,9 +1012,10 @@ __global__ void cg_update_kernel(int N, float2* __restrict__ x, float2* __restri
   if (threadIdx.x == 0) rr_parts[i0] = t;
 }
 
-__global__ void cg_finish_kernel(int N, const double* __restrict__ rr_parts, CgState* __restrict__ st, int iters) {
+__global__ void cg_finish_kernel(int nparts, const double* __restrict__ rr_parts, CgState* __restrict__ st,
+                                 int iters) {
   __shared__ double red[33];
-  const double rho = sum_partials(rr_parts, N, red);
+  const double rho = sum_partials(rr_parts, nparts, red);
   if (threadIdx.x == 0) {
     st->rho[iters] = rho;
     if (!isfinite(rho)) st->finite_ok = 0;
@@ -907,6 +1050,12 @@ static size_t inv_cols_region(const FftArgs& f) {
   const size_t in = sizeof(float2) * static_cast<size_t>(G) * f.C;
   const size_t out = sizeof(float2) * static_cast<size_t>(f.N) * (f.C + 1);
   return align16(std::max({in, out, fft_scratch_bytes<G>(f.C)}));
+}
+// middle stages: [G][C+1] float2 covers the [N][C] / [G][C] slabs and the [N][C+1] output
+template <int G>
+static size_t mid_region(const FftArgs& f) {
+  const size_t rows = sizeof(float2) * static_cast<size_t>(G) * (f.C + 1);
+  return align16(std::max(rows, fft_scratch_bytes<G>(f.C)));
 }
 template <int G>
 static size_t inv_rows_region(const FftArgs& f) {
@@ -974,7 +1123,7 @@ void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, fl
     TSN_FFT_C(f.C, {
       auto k = fwd_rows_kernel<GG, CC>;
       ensure_smem(k, sm);
-      const int grid = persistent_grid(k, 32 * f.C, sm, f.N, f.share);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.lines(), f.share);
       k<<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
     });
   });
@@ -989,8 +1138,38 @@ void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStre
     TSN_FFT_C(f.C, {
       auto k = fwd_cols_kernel<GG, CC>;
       ensure_smem(k, sm);
-      const int grid = persistent_grid(k, 32 * f.C, sm, f.G, f.share);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.gcols(), f.share);
       k<<<grid, 32 * f.C, sm, s>>>(f, z1, panel, static_cast<int>(region), nbuf);
+    });
+  });
+}
+
+void launch_fwd_mid(const FftArgs& f, const float2* z1, float2* z2, cudaStream_t s) {
+  TSN_G_SWITCH(f.G, {
+    const size_t region = mid_region<GG>(f);
+    const size_t base = sizeof(float2) * GG;
+    const int nbuf = base + 2 * region <= kFftTwoCtaSmem ? 2 : 1;
+    const size_t sm = base + nbuf * region;
+    TSN_FFT_C(f.C, {
+      auto k = fwd_mid_kernel<GG, CC>;
+      ensure_smem(k, sm);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.N * f.G, f.share);
+      k<<<grid, 32 * f.C, sm, s>>>(f, z1, z2, static_cast<int>(region), nbuf);
+    });
+  });
+}
+
+void launch_inv_mid(const FftArgs& f, const float2* z2, float2* z1, cudaStream_t s) {
+  TSN_G_SWITCH(f.G, {
+    const size_t region = mid_region<GG>(f);
+    const size_t base = sizeof(float2) * GG;
+    const int nbuf = base + 2 * region <= kFftTwoCtaSmem ? 2 : 1;
+    const size_t sm = base + nbuf * region;
+    TSN_FFT_C(f.C, {
+      auto k = inv_mid_kernel<GG, CC>;
+      ensure_smem(k, sm);
+      const int grid = persistent_grid(k, 32 * f.C, sm, f.N * f.G, f.share);
+      k<<<grid, 32 * f.C, sm, s>>>(f, z2, z1, static_cast<int>(region), nbuf);
     });
   });
 }
@@ -1011,7 +1190,7 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
     TSN_FFT_C(f.C, {
       auto k = inv_cols_kernel<GG, CC>;
       ensure_smem(k, sm);
-      const int g = persistent_grid(k, 32 * f.C, sm, f.G, f.share);
+      const int g = persistent_grid(k, 32 * f.C, sm, f.gcols(), f.share);
       k<<<g, 32 * f.C, sm, s>>>(f, grid, w1, static_cast<int>(region), nbuf);
     });
   });
@@ -1028,21 +1207,29 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
     TSN_FFT_C(f.C, {
       auto k = inv_rows_kernel<GG, CC>;
       ensure_smem(k, sm);
-      const int g = persistent_grid(k, 32 * f.C, sm, f.N, f.share);
+      const int g = persistent_grid(k, 32 * f.C, sm, f.lines(), f.share);
       k<<<g, 32 * f.C, sm, s>>>(f, w1, out, mode, x, r, p, partials, st, iter, inv_scale2, lambda_scaled,
                                 static_cast<int>(region), epi_smem);
     });
   });
 }
 
-void launch_cg_update(int N, float2* x, float2* r, const float2* p, const float2* ap, const double* pap_parts,
-                      double* rr_parts, CgState* st, int iter, cudaStream_t s) {
-  cg_update_kernel<<<N, 256, 0, s>>>(N, x, r, p, ap, pap_parts, rr_parts, st, iter);
+void launch_cg_update(int N, int lines, int nparts, float2* x, float2* r, const float2* p, const float2* ap,
+                      const double* pap_parts, double* rr_parts, CgState* st, int iter, cudaStream_t s) {
+  cg_update_kernel<<<lines, 256, 0, s>>>(N, nparts, x, r, p, ap, pap_parts, rr_parts, st, iter);
 }
 
-void launch_cg_finish(int N, const double* rr_parts, CgState* st, int iters, cudaStream_t s) {
-  cg_finish_kernel<<<1, 256, 0, s>>>(N, rr_parts, st, iters);
+void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters, cudaStream_t s) {
+  cg_finish_kernel<<<1, 256, 0, s>>>(nparts, rr_parts, st, iters);
 }
+
+__global__ void reduce_partials_kernel(double* part, int n) {
+  __shared__ double red[33];
+  const double t = sum_partials(part, n, red);  // every read lands before block_sum's first barrier
+  if (threadIdx.x == 0) part[0] = t;
+}
+
+void launch_reduce_partials(double* part, int n, cudaStream_t s) { reduce_partials_kernel<<<1, 1024, 0, s>>>(part, n); }
 
 template <class T>
 __global__ void gather_rows_kernel(const T* __restrict__ src, const int32_t* __restrict__ map, int64_t rows, int width,

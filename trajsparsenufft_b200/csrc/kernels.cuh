@@ -33,19 +33,23 @@ struct CgState {
 //   [128+576c, +512)         f16 compressed A of component c, [16][16]
 //   [640+576c, +64)          u32 mma.sp pair metadata of component c, [16]
 //   [128+576n, +16)          RecordInfo (n = component count)
-//   [128+576n+16, +48)       24-bit output row of each of the 16 tile rows (little endian,
-//                            0xFFFFFF = pad row)
+//   [128+576n+16, +48)       24-bit output row of each of the 16 tile rows (little endian;
+//                            pad rows are the ones whose live bit in RecordInfo.flags is clear)
 // A one-component record is 768 bytes: records and the gathered rows after them stay on
 // 128-byte boundaries.
 // Work item: a run of at most kChunkTiles tiles of one 16-row group. Groups with more
 // tiles are split; their chunks write raw accumulators to `partials` and the warp that
 // arrives last (counter) sums all chunks in chunk order, so results stay deterministic.
 constexpr int kChunkTiles = 8;
+// A group is cut into at most this many chunks (longer chunks for longer groups), so the
+// warp that reduces a split group reads a bounded number of partials.
+constexpr int kMaxChunks = 64;
 constexpr int kRecInfoBytes = 64;
-constexpr int32_t kRecRowPad = 0xFFFFFF;
-constexpr int64_t kMaxInterpRows = kRecRowPad;  // output rows addressable by a record
-constexpr int kRecFirst = 1;  // first tile of a work item
-constexpr int kRecLast = 2;   // last tile of a work item: apply the epilogue
+constexpr int32_t kRecRowPad = 0xFFFFFF;                      // row field of a pad row
+constexpr int64_t kMaxInterpRows = static_cast<int64_t>(1) << 24;  // output rows addressable by a record
+constexpr int kRecFirst = 1;       // first tile of a work item
+constexpr int kRecLast = 2;        // last tile of a work item: apply the epilogue
+constexpr int kRecLiveShift = 16;  // flags bit 16 + s: tile row s is a real output row
 struct RecordInfo {
   int32_t flags;
   int32_t split;       // -1: whole group; else split-group id (counter index)
@@ -84,9 +88,25 @@ struct InterpOut {
 struct FftArgs {
   int N = 0, G = 0, C = 0, shift = 0;   // grid position n holds image index (n + shift) mod G
   const float2* tw = nullptr;           // exp(-2 pi i e/G), e in [0,G)
-  const float* scaling = nullptr;       // [N][N] deapodization
-  const float2* smaps = nullptr;        // [C][N][N] or null
+  const float* scaling = nullptr;       // [N]^dims deapodization
+  const float2* smaps = nullptr;        // [C][N]^dims or null
   int share = 1;                        // persistent grids use 1/share of the resident CTAs
+  int dims = 2;                         // 2: image [N][N]; 3: volume [N][N][N]
+  // image lines along the last axis (items of the row stages)
+  __host__ __device__ int lines() const { return dims == 3 ? N * N : N; }
+  // pixels (voxels) of one image
+  __host__ __device__ int64_t pix() const { return static_cast<int64_t>(lines()) * N; }
+  // grid lines of the first-axis stages (fwd_cols / inv_cols items)
+  __host__ __device__ int gcols() const { return dims == 3 ? G * G : G; }
+  // divisor applied with the panel scale before the forward FFTs (the transform's gain per
+  // axis is up to G): G for images, G * 2^floor(floor(log2 G) / 2) for volumes; the
+  // interpolation multiplies it back
+  __host__ __device__ float gs() const {
+    if (dims != 3) return static_cast<float>(G);
+    int l = 0;
+    while ((2 << l) <= G) ++l;
+    return static_cast<float>(G) * static_cast<float>(1 << (l / 2));
+  }
 };
 
 void set_twiddle_constants(cudaStream_t s);
@@ -105,18 +125,30 @@ constexpr int kInterpWarpsPerCta = 4;
 
 void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t s);
 
-// forward rows: x (image [N][N] with smaps, coil images [C][N][N] without) -> z1 [G][N][C]
+// Stage layouts (images: i0 slow, i1 fast; volumes: i0, i1, i2; grids in internal rows
+// q1*G + q0 for images, (q2*G + q1)*G + q0 for volumes):
+//   image:  x -rows-> z1 [q1][i0][c] -cols-> panel
+//   volume: x -rows-> z1 [i0][q2][i1][c] -mid-> z2 [q2][q1][i0][c] -cols-> panel
+//   inverse image:  grid -cols-> z1 [q1][i0][c] -rows-> image
+//   inverse volume: grid -cols-> z2 [q2][q1][i0][c] -mid-> z1 [q2][i0][i1][c] -rows-> volume
+// forward rows: x (image with smaps, coil images [C][...] without) -> z1
 // mode 0: plain, sigma from norm partials -> state->sigma_x
 // mode 1: CG iteration k: p = r + beta p (p = r at k == 0), rho_k from rr partials
 // mode 2: CG iteration k after a reliable restart: p = r (beta = 0)
 void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
                      const double* partials, int nparts, CgState* st, int iter, cudaStream_t s);
-// forward columns: z1 -> panel [G*G][4C] (row q1*G + q0), FP16 hi | res
+// forward columns: z1 (z2 for volumes) -> panel [G^dims][4C] in internal rows, FP16 hi | res
 void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStream_t s);
+// forward middle axis of a volume: z1 [i0][q2][i1][c] -> z2 [q2][q1][i0][c]
+void launch_fwd_mid(const FftArgs& f, const float2* z1, float2* z2, cudaStream_t s);
+// inverse middle axis of a volume: z2 [q2][q1][i0][c] -> z1 [q2][i0][i1][c] (crop)
+void launch_inv_mid(const FftArgs& f, const float2* z2, float2* z1, cudaStream_t s);
+// total of n partials into part[0], one CTA in a fixed order
+void launch_reduce_partials(double* part, int n, cudaStream_t s);
 // samples [C][M] (scaled by sigma_y, density) -> sample panel [M][4C]
 void launch_split_samples(const float2* y, const float* density, int64_t m, int c, __half* panel,
                           const double* partials, int nparts, CgState* st, cudaStream_t s);
-// inverse columns: grid [G*G][C] -> w1 [G][N][C]
+// inverse columns: grid [G^dims][C] -> w1 [G][N][C] (images) or z2 (volumes)
 void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStream_t s);
 // inverse rows + crop + deapod + coil combine
 // mode 0: plain adjoint (factor 1/sigma_y): out = [N][N] (smaps) or [C][N][N]
@@ -127,10 +159,11 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
 void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r,
                      const float2* p, double* partials, CgState* st, int iter, float inv_scale2,
                      float lambda_scaled, cudaStream_t s);
-// CG update: x += alpha p, r -= alpha ap, rr partials
-void launch_cg_update(int N, float2* x, float2* r, const float2* p, const float2* ap, const double* pap_parts,
-                      double* rr_parts, CgState* st, int iter, cudaStream_t s);
-void launch_cg_finish(int N, const double* rr_parts, CgState* st, int iters, cudaStream_t s);
+// CG update over `lines` lines of N pixels: x += alpha p, r -= alpha ap, one rr partial per
+// line; alpha from the first `nparts` pAp partials
+void launch_cg_update(int N, int lines, int nparts, float2* x, float2* r, const float2* p, const float2* ap,
+                      const double* pap_parts, double* rr_parts, CgState* st, int iter, cudaStream_t s);
+void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters, cudaStream_t s);
 
 void launch_gather_rows_f16(const __half* src, const int32_t* map, int64_t rows, int width, __half* dst,
                             cudaStream_t s);

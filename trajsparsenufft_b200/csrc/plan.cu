@@ -102,9 +102,10 @@ std::once_flag g_const_once;
 struct tsn_plan {
   tsn_plan_desc desc{};
   int N = 0, G = 0, C = 0, J = 0, ncomp = 0, shift = 0, rowh = 0;
+  int dims = 2;  // 2: [N][N] images on a G^2 grid; 3: [N][N][N] volumes on a G^3 grid
   int64_t M = 0;
   DevView view[2];
-  DeviceBuffer scaling, tw, z1, panel, spanel, grid, r, p, ap, rhs, parts_pap, parts_rr, norm_parts, state;
+  DeviceBuffer scaling, tw, z1, z2, panel, spanel, grid, r, p, ap, rhs, parts_pap, parts_rr, norm_parts, state;
   tsn_plan_info info{};
   std::map<GraphKey, cudaGraphExec_t> graphs;
   ~tsn_plan() {
@@ -133,6 +134,22 @@ namespace {
 
 // reference cell index q0*G + q1 -> internal q1*G + q0
 inline int64_t cell_to_internal(int64_t q, int64_t g) { return (q % g) * g + q / g; }
+// volume cell (q0*G + q1)*G + q2 -> internal (q2*G + q1)*G + q0 (the row the column FFT
+// stage writes: its item q2*G + q1 runs over q0)
+inline int64_t cell_to_internal3(int64_t q, int64_t g) {
+  const int64_t q0 = q / (g * g), q1 = (q / g) % g, q2 = q % g;
+  return (q2 * g + q1) * g + q0;
+}
+inline int64_t to_internal(const tsn_plan* P, int64_t q) {
+  return P->dims == 3 ? cell_to_internal3(q, P->G) : cell_to_internal(q, P->G);
+}
+// pixels (voxels) of one image and grid cells
+inline int64_t image_pixels(const tsn_plan* P) {
+  return static_cast<int64_t>(P->N) * P->N * (P->dims == 3 ? P->N : 1);
+}
+inline int64_t grid_cells(const tsn_plan* P) {
+  return static_cast<int64_t>(P->G) * P->G * (P->dims == 3 ? P->G : 1);
+}
 
 // Bit j set when column j of tile t has a nonzero coefficient in some row of some
 // component.  The others are the planner's padding (stored as column 0 in the pack files)
@@ -184,9 +201,10 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   const int64_t tiles = h.tiles(), groups = h.groups();
   const int ncomp = static_cast<int>(h.a.size());
   const int rec = record_bytes(ncomp);
-  if (h.output_size >= kMaxInterpRows) fail(TSN_ERR_UNSUPPORTED, "too many output rows for 24-bit record rows");
+  if (h.output_size > kMaxInterpRows) fail(TSN_ERR_UNSUPPORTED, "too many output rows for 24-bit record rows");
   // work items: groups of at most kChunkTiles tiles run whole; longer groups are split into
-  // chunks (scheduled first, they are the long poles) reduced in chunk order
+  // at most kMaxChunks chunks (scheduled first, they are the long poles) reduced in chunk
+  // order
   struct Item {
     int32_t group;
     uint32_t t0, t1;
@@ -201,11 +219,11 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
       small.push_back(Item{static_cast<int32_t>(g), a, b, -1, 0, 0, 1});
       continue;
     }
-    const int32_t nch = static_cast<int32_t>((b - a + kChunkTiles - 1) / kChunkTiles);
-    if (nch >= (1 << 15)) fail(TSN_ERR_UNSUPPORTED, "a row group has too many tiles");
+    const uint32_t len = std::max<uint32_t>(kChunkTiles, (b - a + kMaxChunks - 1) / kMaxChunks);
+    const int32_t nch = static_cast<int32_t>((b - a + len - 1) / len);
     for (int32_t k = 0; k < nch; ++k)
-      items.push_back(Item{static_cast<int32_t>(g), a + k * kChunkTiles,
-                           std::min<uint32_t>(b, a + (k + 1) * kChunkTiles), nsplit, slots, k, nch});
+      items.push_back(Item{static_cast<int32_t>(g), a + k * len, std::min<uint32_t>(b, a + (k + 1) * len), nsplit,
+                           slots, k, nch});
     slots += nch;
     ++nsplit;
   }
@@ -222,7 +240,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
       int32_t cols[kKTile];
       for (int j = 0; j < kKTile; ++j) {
         int64_t c = h.tile_col_ids[t * kKTile + j];
-        if (cols_are_cells) c = cell_to_internal(c, P->G);
+        if (cols_are_cells) c = to_internal(P, c);
         cols[j] = ((live >> j) & 1u) ? static_cast<int32_t>(c) : -1;
       }
       std::memcpy(r, cols, sizeof cols);
@@ -237,6 +255,9 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
       }
       RecordInfo info;
       info.flags = (t == it.t0 ? kRecFirst : 0) | (t + 1 == it.t1 ? kRecLast : 0);
+      for (int s = 0; s < kMTile; ++s)
+        if (h.group_row_ids[static_cast<size_t>(it.group) * kMTile + s] >= 0)
+          info.flags |= static_cast<int32_t>(1u << (kRecLiveShift + s));
       info.split = it.split;
       info.first_slot = it.first_slot;
       info.chunk = it.chunk | (it.nchunks << 16);
@@ -244,7 +265,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
       uint8_t* orow = r + 128 + 576 * ncomp + sizeof info;  // 24-bit little-endian rows
       for (int s = 0; s < kMTile; ++s) {
         const int32_t v = h.group_row_ids[static_cast<size_t>(it.group) * kMTile + s];
-        const int64_t row = v < 0 ? kRecRowPad : (rows_are_cells ? cell_to_internal(v, P->G) : v);
+        const int64_t row = v < 0 ? kRecRowPad : (rows_are_cells ? to_internal(P, v) : v);
         for (int k = 0; k < 3; ++k) orow[3 * s + k] = static_cast<uint8_t>((row >> (8 * k)) & 0xFF);
       }
     }
@@ -281,6 +302,9 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
 
 void check_desc(const tsn_plan_desc* d) {
   if (!d) fail(TSN_ERR_ARG, "plan descriptor is NULL");
+  if (d->dims != 0 && d->dims != 2 && d->dims != 3) fail(TSN_ERR_ARG, "dims must be 2 or 3 (0 = 2)");
+  if (d->dims == 3 && static_cast<int64_t>(d->grid_size) * d->grid_size * d->grid_size > kMaxInterpRows)
+    fail(TSN_ERR_UNSUPPORTED, "volume grids are limited to 2^24 cells (G <= 256)");
   if (d->im_size <= 0 || d->im_size % 2 || d->grid_size < d->im_size) fail(TSN_ERR_SHAPE, "need an even image size <= grid size");
   if (d->coils < 4 || d->coils > 16 || d->coils % 4) fail(TSN_ERR_UNSUPPORTED, "coil count must be 4, 8, 12 or 16");
   if (d->kernel_width < 1 || d->kernel_width > 16) fail(TSN_ERR_ARG, "kernel width out of range");
@@ -313,22 +337,32 @@ void allocate_workspaces(tsn_plan* P) {
     tw[e] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
   }
   P->tw.upload(tw);
-  P->z1.alloc(sizeof(float2) * G * N * C);
-  P->panel.alloc(sizeof(__half) * G * G * 4 * C);
+  const int64_t pix = image_pixels(P), cells = grid_cells(P);
+  const int64_t lines = pix / N;  // image lines along the last axis: partials of the row stages
+  if (P->dims == 3) {
+    P->z1.alloc(sizeof(float2) * N * G * N * C);  // [i0][q2][i1][c] and [q2][i0][i1][c]
+    P->z2.alloc(sizeof(float2) * G * G * N * C);  // [q2][q1][i0][c]
+  } else {
+    P->z1.alloc(sizeof(float2) * G * N * C);
+  }
+  P->panel.alloc(sizeof(__half) * cells * 4 * C);
   P->spanel.alloc(sizeof(__half) * std::max<int64_t>(M, 1) * 4 * C);
-  P->grid.alloc(sizeof(float2) * G * G * C);
+  P->grid.alloc(sizeof(float2) * cells * C);
   CUDA_OK(cudaMemset(P->grid.ptr, 0, P->grid.bytes));  // inactive grid rows stay zero
-  P->r.alloc(sizeof(float2) * N * N);
-  P->p.alloc(sizeof(float2) * N * N);
-  P->ap.alloc(sizeof(float2) * N * N);
-  P->rhs.alloc(sizeof(float2) * N * N);
-  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(N, kNormParts));
-  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(N, kNormParts));
+  P->r.alloc(sizeof(float2) * pix);
+  P->p.alloc(sizeof(float2) * pix);
+  P->ap.alloc(sizeof(float2) * pix);
+  P->rhs.alloc(sizeof(float2) * pix);
+  // one partial per line, plus one slot: stage profiling of volumes writes partials at +1 so
+  // the solve's totals in slot 0 stay readable
+  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(lines + 1, kNormParts));
+  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(lines + 1, kNormParts));
   P->norm_parts.alloc(sizeof(double) * kNormParts);
   P->state.alloc(sizeof(CgState));
   CUDA_OK(cudaMemset(P->state.ptr, 0, sizeof(CgState)));
-  P->info.workspace_bytes = static_cast<int64_t>(P->z1.bytes + P->panel.bytes + P->spanel.bytes + P->grid.bytes +
-                                                 3 * P->r.bytes + P->state.bytes);
+  P->info.dims = P->dims;
+  P->info.workspace_bytes = static_cast<int64_t>(P->z1.bytes + P->z2.bytes + P->panel.bytes + P->spanel.bytes +
+                                                 P->grid.bytes + 4 * P->r.bytes + P->state.bytes);
   std::call_once(g_const_once, []() { set_twiddle_constants(nullptr); });
   CUDA_OK(cudaGetLastError());
 }
@@ -343,7 +377,39 @@ FftArgs fft_args(const tsn_plan* P, const void* smaps, int share = 1) {
   f.tw = P->tw.as<float2>();
   f.scaling = P->scaling.as<float>();
   f.smaps = static_cast<const float2*>(smaps);
+  f.dims = P->dims;
   return f;
+}
+
+// Forward FFT chain, image (or coil images) -> grid panel: rows, then (volumes) the middle
+// axis, then the first axis into the panel.
+void fwd_chain(tsn_plan* P, const FftArgs& f, const float2* x, int mode, float2* p, const float2* r,
+               const double* parts, int nparts, CgState* st, int iter, __half* panel, cudaStream_t s) {
+  launch_fwd_rows(f, x, P->z1.as<float2>(), mode, p, r, parts, nparts, st, iter, s);
+  if (P->dims == 3) {
+    launch_fwd_mid(f, P->z1.as<float2>(), P->z2.as<float2>(), s);
+    launch_fwd_cols(f, P->z2.as<float2>(), panel, s);
+  } else {
+    launch_fwd_cols(f, P->z1.as<float2>(), panel, s);
+  }
+}
+
+// Inverse FFT chain up to the row stage's input (z1): first axis, then (volumes) the middle.
+void inv_to_lines(tsn_plan* P, const FftArgs& f, const float2* grid, cudaStream_t s) {
+  if (P->dims == 3) {
+    launch_inv_cols(f, grid, P->z2.as<float2>(), s);
+    launch_inv_mid(f, P->z2.as<float2>(), P->z1.as<float2>(), s);
+  } else {
+    launch_inv_cols(f, grid, P->z1.as<float2>(), s);
+  }
+}
+
+// Partials written per image line are summed once for volumes (N^2 of them would be re-read
+// by every CTA of the next stage); returns how many partials the consumer reads.
+int settle_partials(const tsn_plan* P, double* parts, cudaStream_t s) {
+  if (P->dims != 3) return P->N;
+  launch_reduce_partials(parts, static_cast<int>(image_pixels(P) / P->N), s);
+  return 1;
 }
 
 HostView host_view_from_dirs(const char* real_dir, const char* imag_dir) {
@@ -390,6 +456,50 @@ HostView host_view_from_tiles(const SparseView& structure, const std::vector<con
     h.a.push_back(ct.values);
     h.meta.push_back(ct.pair_meta);
   }
+  return h;
+}
+
+// One component view packed and compressed in batches of row groups: the unpacked tiles of
+// one batch at a time (a few hundred MB) instead of the whole view, which for a 256^3 grid
+// would need tens of GB of host memory. The tiles are those of pack_view (same row order,
+// same per-group seeds); the fast and optimized planners emit legal tiles only.
+constexpr int64_t kVolumeFastUnion = 2048;  // column union above which a group is packed the fast way
+HostView host_view_batched(const SparseView& v, const tsn_plan_desc* d) {
+  if (d->planner != TSN_PLANNER_FAST && d->planner != TSN_PLANNER_OPTIMIZED)
+    fail(TSN_ERR_UNSUPPORTED, "volume plans use the fast or optimized planner");
+  const std::vector<int64_t> order = row_order(v, d->policy, kKTile);
+  const int64_t n_groups = (static_cast<int64_t>(order.size()) + kMTile - 1) / kMTile;
+  HostView h;
+  h.output_size = v.output_size;
+  h.n_cols = v.n_cols;
+  h.active_rows = v.rows();
+  h.nnz = v.nnz();
+  h.a.resize(1);
+  h.meta.resize(1);
+  constexpr int64_t kBatchGroups = 8192;
+  int32_t prev[kMTile];
+  bool have_prev = false;
+  for (int64_t g0 = 0; g0 < n_groups; g0 += kBatchGroups) {
+    const int64_t g1 = std::min(n_groups, g0 + kBatchGroups);
+    const std::vector<PackTile> tiles =
+        pack_groups(v, order, g0, g1, d->planner, kKTile, d->seed, d->threads, kVolumeFastUnion);
+    const size_t base = h.tile_col_ids.size() / kKTile;
+    for (size_t i = 0; i < tiles.size(); ++i) {
+      const PackTile& tl = tiles[i];
+      if (!legal_24(tl)) fail(TSN_ERR_FORMAT, "planner emitted an illegal 2:4 tile");
+      if (!have_prev || std::memcmp(prev, tl.row_ids, sizeof prev) != 0) {  // a group starts here
+        h.group_offsets.push_back(static_cast<uint32_t>(base + i));
+        h.group_row_ids.insert(h.group_row_ids.end(), tl.row_ids, tl.row_ids + kMTile);
+        std::memcpy(prev, tl.row_ids, sizeof prev);
+        have_prev = true;
+      }
+    }
+    const CompressedTiles ct = compress_tiles(tiles);
+    h.tile_col_ids.insert(h.tile_col_ids.end(), ct.col_ids.begin(), ct.col_ids.end());
+    h.a[0].insert(h.a[0].end(), ct.values.begin(), ct.values.end());
+    h.meta[0].insert(h.meta[0].end(), ct.pair_meta.begin(), ct.pair_meta.end());
+  }
+  h.group_offsets.push_back(static_cast<uint32_t>(h.tile_col_ids.size() / kKTile));
   return h;
 }
 
@@ -440,6 +550,7 @@ tsn_status tsn_plan_create_from_pack(const char* fwd_real, const char* fwd_imag,
     if (!out) fail(TSN_ERR_ARG, "plan output pointer is NULL");
     *out = nullptr;
     check_desc(desc);
+    if (desc->dims == 3) fail(TSN_ERR_UNSUPPORTED, "pack directories hold image (2D) views");
     if (!fwd_real && !adj_real) fail(TSN_ERR_ARG, "at least one view directory is required");
     const auto t0 = std::chrono::steady_clock::now();
     std::unique_ptr<tsn_plan> P(new tsn_plan);
@@ -506,11 +617,61 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
     P->C = desc->coils;
     P->J = desc->kernel_width;
     P->M = m;
+    P->dims = desc->dims == 3 ? 3 : 2;
     const bool reference_layout = (desc->flags & TSN_FLAG_REFERENCE_LAYOUT) != 0;
     P->shift = reference_layout ? 0 : P->N / 2;
-    for (int64_t i = 0; i < 2 * m; ++i)
+    for (int64_t i = 0; i < P->dims * m; ++i)
       if (!std::isfinite(traj[i]) || std::fabs(traj[i]) > 0.500001f)
         fail(TSN_ERR_ARG, "trajectory must use normalized [-0.5, 0.5] coordinates");
+    if (P->dims == 3) {
+      // volume: real KB weights on the centred layout, views packed in batches
+      if (reference_layout) fail(TSN_ERR_UNSUPPORTED, "volume plans use the centred layout (real KB weights)");
+      if (m > kMaxInterpRows) fail(TSN_ERR_UNSUPPORTED, "a volume plan holds at most 2^24 samples");
+      KbCsr kb = kb_weights_csr3(traj, m, P->N, P->G, P->J, desc->threads);
+      HostView hv[2];
+      {
+        SparseView w_g;
+        w_g.dims = 3;
+        w_g.output_size = m;
+        w_g.n_cols = static_cast<int64_t>(P->G) * P->G * P->G;
+        w_g.row_ptr = std::move(kb.row_ptr);
+        w_g.cols = std::move(kb.cols);
+        w_g.vals = std::move(kb.re);
+        w_g.row_ids.resize(m);
+        w_g.coords.resize(3 * m);
+        const double g = P->G;
+        for (int64_t i = 0; i < m; ++i) {
+          w_g.row_ids[i] = i;
+          for (int d = 0; d < 3; ++d) w_g.coords[3 * i + d] = np_mod(static_cast<double>(traj[3 * i + d]) * g + g / 2.0, g);
+        }
+        hv[0] = host_view_batched(w_g, desc);
+        const SparseView w_gt = transpose_view(w_g, P->G);
+        w_g = SparseView();
+        hv[1] = host_view_batched(w_gt, desc);
+      }
+      P->ncomp = 1;
+      const auto d3 = deapodization3(P->N, P->G, P->J);
+      std::vector<float> sc(d3.size());
+      for (size_t i = 0; i < sc.size(); ++i) sc[i] = static_cast<float>(d3[i]);
+      CUDA_OK(cudaSetDevice(desc->device));
+      P->scaling.upload(sc);
+      P->info.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
+      hv[0] = HostView();
+      upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
+      hv[1] = HostView();
+      allocate_workspaces(P.get());
+      P->info.samples = P->M;
+      P->info.im_size = P->N;
+      P->info.grid_size = P->G;
+      P->info.coils = P->C;
+      P->info.kernel_width = P->J;
+      P->info.components = P->ncomp;
+      P->info.interp = TSN_INTERP_MMA_SP;
+      P->info.dims = 3;
+      *out = P.release();
+      return TSN_OK;
+    }
     const KbCsr kb = kb_interpolation_csr(traj, m, P->N, P->G, P->J);
     std::vector<double> ones(kb.cols.size(), 1.0), weights(kb.cols.size());
     for (size_t i = 0; i < weights.size(); ++i) weights[i] = std::hypot(kb.re[i], kb.im[i]);
@@ -549,6 +710,7 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
     P->info.kernel_width = P->J;
     P->info.components = P->ncomp;
     P->info.interp = TSN_INTERP_MMA_SP;
+    P->info.dims = 2;
     *out = P.release();
     return TSN_OK;
   } catch (const std::exception& e) {
@@ -586,18 +748,17 @@ void need_views(const tsn_plan* P, bool fwd, bool adj) {
 void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cudaStream_t s) {
   const FftArgs f = fft_args(P, smaps);
   CgState* st = P->state.as<CgState>();
-  const int64_t n = static_cast<int64_t>(P->N) * P->N * (smaps ? 1 : P->C);
+  const int64_t n = image_pixels(P) * (smaps ? 1 : P->C);
   launch_norm_partials(static_cast<const float2*>(x), n, P->norm_parts.as<double>(), s);
-  launch_fwd_rows(f, static_cast<const float2*>(x), P->z1.as<float2>(), 0, nullptr, nullptr, P->norm_parts.as<double>(),
-                  kNormParts, st, 0, s);
-  launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
+  fwd_chain(P, f, static_cast<const float2*>(x), 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0,
+            P->panel.as<__half>(), s);
   InterpOut o;
   o.c64 = static_cast<float2*>(y);
   o.rows = P->M;
   o.coils = P->C;
   o.scale_ptr = &st->sigma_x;
   o.scale_inv = 1;
-  o.scale_mul = static_cast<float>(P->G);
+  o.scale_mul = f.gs();
   launch_interp(P->view[TSN_VIEW_G].v, P->panel.as<__half>(), P->rowh, true, EPI_SAMPLES, false, o, s);
 }
 
@@ -629,7 +790,7 @@ void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cuda
                        P->norm_parts.as<double>(), kNormParts, st, s);
   InterpOut o;
   o.c64 = P->grid.as<float2>();
-  o.rows = static_cast<int64_t>(P->G) * P->G;
+  o.rows = grid_cells(P);
   o.coils = P->C;
   launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, o, s);
 }
@@ -648,16 +809,17 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
   float2* X = static_cast<float2*>(x);
   float2 *R = P->r.as<float2>(), *Pv = P->p.as<float2>(), *AP = P->ap.as<float2>();
   double *pap = P->parts_pap.as<double>(), *rr = P->parts_rr.as<double>();
+  const int lines = f.lines();
   enqueue_adjoint_grid(P, y, density, s, share);
-  launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
+  inv_to_lines(P, f, P->grid.as<float2>(), s);
   launch_inv_rows(f, P->z1.as<float2>(), nullptr, 1, X, R, nullptr, rr, st, 0, inv_s2, 0.f, s);
+  int n_rr = settle_partials(P, rr, s);
   if (reliable_period > 0)  // keep b for the reliable residuals
     CUDA_OK(cudaMemcpyAsync(P->rhs.ptr, R, P->rhs.bytes, cudaMemcpyDeviceToDevice, s));
   bool restart = false;
   for (int k = 0; k < iters; ++k) {
-    launch_fwd_rows(f, nullptr, P->z1.as<float2>(), restart ? 2 : 1, Pv, R, rr, P->N, st, k, s);
+    fwd_chain(P, f, nullptr, restart ? 2 : 1, Pv, R, rr, n_rr, st, k, P->panel.as<__half>(), s);
     restart = false;
-    launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
     InterpOut of;
     of.panel = P->spanel.as<__half>();
     of.density = density;
@@ -666,25 +828,27 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     launch_interp(interp_view(P, TSN_VIEW_G, share), P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
     InterpOut oa;
     oa.c64 = P->grid.as<float2>();
-    oa.rows = static_cast<int64_t>(P->G) * P->G;
+    oa.rows = grid_cells(P);
     oa.coils = P->C;
     launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
-    launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
+    inv_to_lines(P, f, P->grid.as<float2>(), s);
     launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, k, inv_s2, lam, s);
-    launch_cg_update(P->N, X, R, Pv, AP, pap, rr, st, k, s);
+    const int n_pap = settle_partials(P, pap, s);
+    launch_cg_update(P->N, lines, n_pap, X, R, Pv, AP, pap, rr, st, k, s);
+    n_rr = settle_partials(P, rr, s);
     if (reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters) {
       // r = b - (A^H W A + lambda) x: plain forward of x, then the adjoint into residual mode
-      launch_norm_partials(X, static_cast<int64_t>(P->N) * P->N, P->norm_parts.as<double>(), s);
-      launch_fwd_rows(f, X, P->z1.as<float2>(), 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, s);
-      launch_fwd_cols(f, P->z1.as<float2>(), P->panel.as<__half>(), s);
+      launch_norm_partials(X, image_pixels(P), P->norm_parts.as<double>(), s);
+      fwd_chain(P, f, X, 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, P->panel.as<__half>(), s);
       launch_interp(interp_view(P, TSN_VIEW_G, share), P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
       launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
-      launch_inv_cols(f, P->grid.as<float2>(), P->z1.as<float2>(), s);
+      inv_to_lines(P, f, P->grid.as<float2>(), s);
       launch_inv_rows(f, P->z1.as<float2>(), R, 3, P->rhs.as<float2>(), nullptr, X, rr, st, k, inv_s2, lam, s);
+      n_rr = settle_partials(P, rr, s);
       restart = reliable_direction == 0;
     }
   }
-  launch_cg_finish(P->N, rr, st, iters, s);
+  launch_cg_finish(n_rr, rr, st, iters, s);
 }
 
 // Reads a finished solve's scalar state (synchronizes s) into the optional host outputs and
@@ -712,7 +876,7 @@ tsn_status read_cg_state(const tsn_plan* P, int iters, double* residual_history,
 // Rough cost of one CG iteration of a plan in tile units (sparse tiles plus FFT points).
 double case_cost(const tsn_plan* P) {
   return static_cast<double>(P->view[TSN_VIEW_G].tiles + P->view[TSN_VIEW_GT].tiles) +
-         static_cast<double>(P->C) * P->G * P->G / 25.0;
+         static_cast<double>(P->C) * static_cast<double>(grid_cells(P)) / 25.0;
 }
 
 }  // namespace
@@ -740,7 +904,7 @@ tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     enqueue_adjoint_grid(plan, y, nullptr, s);
     const FftArgs f = fft_args(plan, smaps);
-    launch_inv_cols(f, plan->grid.as<float2>(), plan->z1.as<float2>(), s);
+    inv_to_lines(plan, f, plan->grid.as<float2>(), s);
     launch_inv_rows(f, plan->z1.as<float2>(), static_cast<float2*>(x), 0, nullptr, nullptr, nullptr, nullptr,
                     plan->state.as<CgState>(), 0, 1.0f, 0.f, s);
     CUDA_OK(cudaGetLastError());
@@ -953,8 +1117,11 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
     need_views(plan, true, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     DeviceBuffer xbuf;
-    xbuf.alloc(sizeof(float2) * plan->N * plan->N);
+    xbuf.alloc(sizeof(float2) * image_pixels(plan));
     enqueue_cg(plan, y, smaps, nullptr, 1e-4f, 1.0f, 2, xbuf.ptr, s);
+    const bool vol = plan->dims == 3;
+    const int nparts = vol ? 1 : plan->N;  // the solve left single totals for volumes
+    float2* z_cols = vol ? plan->z2.as<float2>() : plan->z1.as<float2>();  // first-axis stage data
     const FftArgs f = fft_args(plan, smaps);
     CgState* st = plan->state.as<CgState>();
     float2 *X = xbuf.as<float2>(), *R = plan->r.as<float2>(), *Pv = plan->p.as<float2>(), *AP = plan->ap.as<float2>();
@@ -962,8 +1129,14 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
     // iteration index 1 keeps p = r + beta p live; the stages read state written by the solve
     auto stage = [&](int which) {
       switch (which) {
-        case TSN_STAGE_FWD_ROWS: launch_fwd_rows(f, nullptr, plan->z1.as<float2>(), 1, Pv, R, rr, plan->N, st, 1, s); break;
-        case TSN_STAGE_FWD_COLS: launch_fwd_cols(f, plan->z1.as<float2>(), plan->panel.as<__half>(), s); break;
+        case TSN_STAGE_FWD_ROWS: launch_fwd_rows(f, nullptr, plan->z1.as<float2>(), 1, Pv, R, rr, nparts, st, 1, s); break;
+        case TSN_STAGE_FWD_COLS: launch_fwd_cols(f, z_cols, plan->panel.as<__half>(), s); break;
+        case TSN_STAGE_FWD_MID:
+          if (vol) launch_fwd_mid(f, plan->z1.as<float2>(), plan->z2.as<float2>(), s);
+          break;
+        case TSN_STAGE_INV_MID:
+          if (vol) launch_inv_mid(f, plan->z2.as<float2>(), plan->z1.as<float2>(), s);
+          break;
         case TSN_STAGE_INTERP_FWD: {
           InterpOut o;
           o.panel = plan->spanel.as<__half>();
@@ -974,21 +1147,27 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
         case TSN_STAGE_INTERP_ADJ: {
           InterpOut o;
           o.c64 = plan->grid.as<float2>();
-          o.rows = static_cast<int64_t>(plan->G) * plan->G;
+          o.rows = grid_cells(plan);
           o.coils = plan->C;
           launch_interp(plan->view[TSN_VIEW_GT].v, plan->spanel.as<__half>(), plan->rowh, true, EPI_GRID, true, o, s);
         } break;
-        case TSN_STAGE_INV_COLS: launch_inv_cols(f, plan->grid.as<float2>(), plan->z1.as<float2>(), s); break;
+        case TSN_STAGE_INV_COLS: launch_inv_cols(f, plan->grid.as<float2>(), z_cols, s); break;
         case TSN_STAGE_INV_ROWS:
-          launch_inv_rows(f, plan->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, 1, 1.0f, 1e-4f, s);
+          // volumes: partials stay per line here; cg_update below reads the solve's total
+          launch_inv_rows(f, plan->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, vol ? rr + 1 : pap, st, 1, 1.0f,
+                          1e-4f, s);
           break;
-        default: launch_cg_update(plan->N, X, R, Pv, AP, pap, rr, st, 1, s); break;
+        default: launch_cg_update(plan->N, f.lines(), nparts, X, R, Pv, AP, pap, vol ? rr + 1 : rr, st, 1, s); break;
       }
     };
     cudaEvent_t e0, e1;
     CUDA_OK(cudaEventCreate(&e0));
     CUDA_OK(cudaEventCreate(&e1));
     for (int which = 0; which < TSN_STAGE_COUNT; ++which) {
+      if (!vol && (which == TSN_STAGE_FWD_MID || which == TSN_STAGE_INV_MID)) {
+        stage_ms[which] = 0.0;  // images have no middle axis
+        continue;
+      }
       stage(which);  // warm
       CUDA_OK(cudaEventRecord(e0, s));
       for (int r = 0; r < reps; ++r) stage(which);
@@ -1016,17 +1195,16 @@ tsn_status tsn_fft_forward_panel(tsn_plan* plan, const void* x, const void* smap
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const FftArgs f = fft_args(plan, smaps);
     CgState* st = plan->state.as<CgState>();
-    const int64_t n = static_cast<int64_t>(plan->N) * plan->N * (smaps ? 1 : plan->C);
+    const int64_t n = image_pixels(plan) * (smaps ? 1 : plan->C);
     launch_norm_partials(static_cast<const float2*>(x), n, plan->norm_parts.as<double>(), s);
-    launch_fwd_rows(f, static_cast<const float2*>(x), plan->z1.as<float2>(), 0, nullptr, nullptr,
-                    plan->norm_parts.as<double>(), kNormParts, st, 0, s);
-    launch_fwd_cols(f, plan->z1.as<float2>(), static_cast<__half*>(panel_f16), s);
+    fwd_chain(plan, f, static_cast<const float2*>(x), 0, nullptr, nullptr, plan->norm_parts.as<double>(), kNormParts,
+              st, 0, static_cast<__half*>(panel_f16), s);
     CUDA_OK(cudaGetLastError());
     if (panel_scale) {
       float sigma = 0.f;
       CUDA_OK(cudaMemcpyAsync(&sigma, &st->sigma_x, sizeof(float), cudaMemcpyDeviceToHost, s));
       CUDA_OK(cudaStreamSynchronize(s));
-      *panel_scale = sigma / static_cast<float>(plan->G);
+      *panel_scale = sigma / f.gs();
     }
     return TSN_OK;
   } catch (const std::exception& e) {
@@ -1046,7 +1224,7 @@ tsn_status tsn_fft_adjoint_image(tsn_plan* plan, const void* grid_c64, const voi
     // unit sample scale for the plain adjoint epilogue (factor = 1 / sigma_y)
     const float one = 1.0f;
     CUDA_OK(cudaMemcpyAsync(&st->sigma_y, &one, sizeof(float), cudaMemcpyHostToDevice, s));
-    launch_inv_cols(f, static_cast<const float2*>(grid_c64), plan->z1.as<float2>(), s);
+    inv_to_lines(plan, f, static_cast<const float2*>(grid_c64), s);
     launch_inv_rows(f, plan->z1.as<float2>(), static_cast<float2*>(x), 0, nullptr, nullptr, nullptr, nullptr, st, 0,
                     1.0f, 0.f, s);
     CUDA_OK(cudaGetLastError());

@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cmath>
 #include <limits>
+#include <memory>
 #include <thread>
 #include <unordered_map>
 
@@ -56,7 +57,78 @@ static void parallel_for(int64_t n, int threads, F&& body) {
   if (err) std::rethrow_exception(err);
 }
 
+// Volume transpose on all host cores: atomic cell counts, an atomic scatter, then each row's
+// entries sorted by source row, which gives exactly the serial transpose's layout (a
+// sample touches a cell at most once).
+static SparseView transpose_view_parallel(const SparseView& v, int64_t grid_size) {
+  const int threads = resolve_threads(0);
+  const int64_t n_rows = v.rows();
+  const int64_t blocks = (n_rows + 4095) / 4096;
+  std::unique_ptr<std::atomic<int32_t>[]> count(new std::atomic<int32_t>[v.n_cols]);
+  for (int64_t c = 0; c < v.n_cols; ++c) count[c].store(0, std::memory_order_relaxed);
+  std::atomic<bool> bad{false};
+  parallel_for(blocks, threads, [&](int64_t b) {
+    const int64_t r1 = std::min(n_rows, (b + 1) * 4096);
+    for (int64_t k = v.row_ptr[b * 4096]; k < v.row_ptr[r1]; ++k) {
+      const int64_t c = v.cols[k];
+      if (c < 0 || c >= v.n_cols) {
+        bad.store(true);
+        return;
+      }
+      count[c].fetch_add(1, std::memory_order_relaxed);
+    }
+  });
+  if (bad.load()) fail(TSN_ERR_SHAPE, "column id out of range");
+  SparseView t;
+  t.output_size = v.n_cols;
+  t.n_cols = v.output_size;
+  t.dims = v.dims;
+  std::unique_ptr<std::atomic<int64_t>[]> cursor(new std::atomic<int64_t>[v.n_cols]);
+  t.row_ptr.push_back(0);
+  for (int64_t c = 0; c < v.n_cols; ++c) {
+    const int32_t n = count[c].load(std::memory_order_relaxed);
+    cursor[c].store(t.row_ptr.back(), std::memory_order_relaxed);
+    if (!n) continue;
+    t.row_ids.push_back(c);
+    t.coords.push_back(static_cast<double>(c % grid_size));
+    t.coords.push_back(static_cast<double>((c / grid_size) % grid_size));
+    t.coords.push_back(static_cast<double>(c / (grid_size * grid_size)));
+    t.row_ptr.push_back(t.row_ptr.back() + n);
+  }
+  count.reset();
+  t.cols.resize(v.nnz());
+  t.vals.resize(v.nnz());
+  parallel_for(blocks, threads, [&](int64_t b) {
+    const int64_t r0 = b * 4096, r1 = std::min(n_rows, r0 + 4096);
+    for (int64_t r = r0; r < r1; ++r) {
+      const int64_t logical = v.row_ids[r];
+      for (int64_t k = v.row_ptr[r]; k < v.row_ptr[r + 1]; ++k) {
+        const int64_t at = cursor[v.cols[k]].fetch_add(1, std::memory_order_relaxed);
+        t.cols[at] = logical;
+        t.vals[at] = v.vals[k];
+      }
+    }
+  });
+  cursor.reset();
+  const int64_t out_rows = t.rows();
+  parallel_for((out_rows + 1023) / 1024, threads, [&](int64_t b) {
+    std::vector<std::pair<int64_t, double>> tmp;
+    for (int64_t r = b * 1024; r < std::min(out_rows, (b + 1) * 1024); ++r) {
+      const int64_t a = t.row_ptr[r], e = t.row_ptr[r + 1];
+      tmp.clear();
+      for (int64_t k = a; k < e; ++k) tmp.emplace_back(t.cols[k], t.vals[k]);
+      std::sort(tmp.begin(), tmp.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+      for (int64_t k = a; k < e; ++k) {
+        t.cols[k] = tmp[k - a].first;
+        t.vals[k] = tmp[k - a].second;
+      }
+    }
+  });
+  return t;
+}
+
 SparseView transpose_view(const SparseView& v, int64_t grid_size) {
+  if (v.dims == 3) return transpose_view_parallel(v, grid_size);
   std::vector<int64_t> count(v.n_cols, 0);
   for (int64_t c : v.cols) {
     if (c < 0 || c >= v.n_cols) fail(TSN_ERR_SHAPE, "column id out of range");
@@ -65,6 +137,7 @@ SparseView transpose_view(const SparseView& v, int64_t grid_size) {
   SparseView t;
   t.output_size = v.n_cols;
   t.n_cols = v.output_size;
+  t.dims = v.dims;
   std::vector<int64_t> slot(v.n_cols, -1);
   t.row_ptr.push_back(0);
   for (int64_t c = 0; c < v.n_cols; ++c) {
@@ -72,7 +145,8 @@ SparseView transpose_view(const SparseView& v, int64_t grid_size) {
     slot[c] = static_cast<int64_t>(t.row_ids.size());
     t.row_ids.push_back(c);
     t.coords.push_back(static_cast<double>(c % grid_size));
-    t.coords.push_back(static_cast<double>(c / grid_size));
+    t.coords.push_back(static_cast<double>((c / grid_size) % (v.dims == 3 ? grid_size : INT64_MAX)));
+    if (v.dims == 3) t.coords.push_back(static_cast<double>(c / (grid_size * grid_size)));
     t.row_ptr.push_back(t.row_ptr.back() + count[c]);
   }
   std::vector<int64_t> fill(t.row_ids.size(), 0);
@@ -99,6 +173,13 @@ static uint32_t spread16(uint32_t v) {
   return v;
 }
 
+// 3D morton: bit b of v goes to bit 3b.
+static uint64_t spread21(uint32_t v) {
+  uint64_t out = 0;
+  for (int b = 0; b < 21; ++b) out |= static_cast<uint64_t>((v >> b) & 1u) << (3 * b);
+  return out;
+}
+
 // Python int(round(x)): round half to even.
 static int64_t py_round(double x) { return static_cast<int64_t>(std::nearbyint(x)); }
 
@@ -110,11 +191,22 @@ std::vector<int64_t> row_order(const SparseView& v, int policy, int k_tile) {
   for (int64_t i = 0; i < n; ++i) order[i] = i;
   if (policy == TSN_POLICY_TRAJECTORY) return order;
   std::vector<uint64_t> key(n);
-  for (int64_t r = 0; r < n; ++r) {
-    const int64_t x = std::max<int64_t>(0, py_round(v.coords[2 * r]));
-    const int64_t y = std::max<int64_t>(0, py_round(v.coords[2 * r + 1]));
-    key[r] = static_cast<uint64_t>(spread16(static_cast<uint32_t>(x & 0xFFFF))) |
-             (static_cast<uint64_t>(spread16(static_cast<uint32_t>(y & 0xFFFF))) << 1);
+  if (v.dims == 3) {
+    for (int64_t r = 0; r < n; ++r) {
+      uint64_t k = 0;
+      for (int d = 0; d < 3; ++d) {
+        const int64_t c = std::max<int64_t>(0, py_round(v.coords[3 * r + d]));
+        k |= spread21(static_cast<uint32_t>(c & 0x1FFFFF)) << d;
+      }
+      key[r] = k;
+    }
+  } else {
+    for (int64_t r = 0; r < n; ++r) {
+      const int64_t x = std::max<int64_t>(0, py_round(v.coords[2 * r]));
+      const int64_t y = std::max<int64_t>(0, py_round(v.coords[2 * r + 1]));
+      key[r] = static_cast<uint64_t>(spread16(static_cast<uint32_t>(x & 0xFFFF))) |
+               (static_cast<uint64_t>(spread16(static_cast<uint32_t>(y & 0xFFFF))) << 1);
+    }
   }
   std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
   if (policy == TSN_POLICY_MORTON) return order;
@@ -466,6 +558,40 @@ void materialize(const SparseView& v, const int64_t* local_rows, const std::vect
   }
 }
 
+// materialize for a tile whose column ids are an ascending run (then -1 pads), over rows whose
+// CSR columns ascend without repeats: one binary search per row instead of a scan of the
+// whole row (rows next to the centre of a 3D radial trajectory hold tens of thousands).
+void materialize_run(const SparseView& v, const int64_t* local_rows, const std::vector<int64_t>& cols, int k_tile,
+                     PackTile& t) {
+  t.col_ids.assign(k_tile, -1);
+  int nlive = 0;
+  for (int j = 0; j < k_tile; ++j) {
+    t.col_ids[j] = static_cast<int32_t>(cols[j]);
+    if (cols[j] >= 0) nlive = j + 1;
+  }
+  t.values.assign(static_cast<size_t>(kMTile) * k_tile, 0.0);
+  for (int slot = 0; slot < kMTile; ++slot) {
+    const int64_t r = local_rows[slot];
+    t.row_ids[slot] = r >= 0 ? static_cast<int32_t>(v.row_ids[r]) : -1;
+    if (r < 0 || nlive == 0) continue;
+    const int64_t* base = v.cols.data();
+    const int64_t* it = std::lower_bound(base + v.row_ptr[r], base + v.row_ptr[r + 1], cols[0]);
+    const int64_t* end = base + v.row_ptr[r + 1];
+    int j = 0;
+    while (it != end && j < nlive) {
+      if (*it < cols[j]) {
+        ++it;
+      } else if (*it > cols[j]) {
+        ++j;
+      } else {
+        t.values[static_cast<size_t>(slot) * k_tile + j] = v.vals[it - base];
+        ++it;
+        ++j;
+      }
+    }
+  }
+}
+
 void split_illegal(const PackTile& t, PackTile& l0, PackTile& l1) {
   const int k = static_cast<int>(t.col_ids.size());
   l0 = t;
@@ -510,16 +636,26 @@ std::vector<PackTile> pack_view(const SparseView& v, int planner, int policy, in
     fail(TSN_ERR_ARG, "fast/optimized planners use K32 tiles");
   const std::vector<int64_t> order = row_order(v, policy, k_tile);
   const int64_t n_groups = ceil_div(static_cast<int64_t>(order.size()), kMTile);
-  std::vector<std::vector<PackTile>> per_group(n_groups);
-  parallel_for(n_groups, resolve_threads(threads), [&](int64_t gi) {
+  return pack_groups(v, order, 0, n_groups, planner, k_tile, seed, threads, 0);
+}
+
+std::vector<PackTile> pack_groups(const SparseView& v, const std::vector<int64_t>& order, int64_t g0,
+                                  int64_t g1, int planner, int k_tile, uint64_t seed, int threads,
+                                  int64_t fast_above) {
+  std::vector<std::vector<PackTile>> per_group(std::max<int64_t>(g1 - g0, 0));
+  parallel_for(g1 - g0, resolve_threads(threads), [&](int64_t li) {
+    const int64_t gi = g0 + li;
     int64_t rows[kMTile];
     for (int s = 0; s < kMTile; ++s) {
       const int64_t at = gi * kMTile + s;
       rows[s] = at < static_cast<int64_t>(order.size()) ? order[at] : -1;
     }
-    auto& out = per_group[gi];
+    auto& out = per_group[li];
     const uint64_t gseed = seed + static_cast<uint64_t>(gi) * 1009u;
-    if (planner == TSN_PLANNER_FAST) {
+    const bool optimized = planner == TSN_PLANNER_OPTIMIZED;
+    const Masks m = (planner == TSN_PLANNER_FAST) ? Masks{} : column_masks(v, rows);
+    if (planner == TSN_PLANNER_FAST ||
+        (optimized && fast_above > 0 && static_cast<int64_t>(m.cols.size()) > fast_above)) {
       std::vector<int64_t> uni;
       for (int s = 0; s < kMTile; ++s)
         if (rows[s] >= 0)
@@ -530,7 +666,8 @@ std::vector<PackTile> pack_view(const SparseView& v, int planner, int policy, in
         std::vector<int64_t> cols(kKTile, -1);
         for (size_t j = 0; j < kKTile && off + j < uni.size(); ++j) cols[j] = uni[off + j];
         PackTile t;
-        materialize(v, rows, cols, kKTile, t);
+        if (fast_above > 0) materialize_run(v, rows, cols, kKTile, t);
+        else materialize(v, rows, cols, kKTile, t);
         t.legal = legal_24(t);
         if (t.legal) {
           out.push_back(std::move(t));
@@ -543,8 +680,6 @@ std::vector<PackTile> pack_view(const SparseView& v, int planner, int policy, in
       }
       return;
     }
-    const bool optimized = planner == TSN_PLANNER_OPTIMIZED;
-    const Masks m = column_masks(v, rows);
     const auto tiles = assign_columns(m, k_tile, gseed, optimized);
     for (size_t ti = 0; ti < tiles.size(); ++ti) {
       bool legal = true;

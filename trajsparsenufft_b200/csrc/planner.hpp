@@ -23,14 +23,16 @@ struct SparseView {
   std::vector<int64_t> row_ptr;  // rows + 1
   std::vector<int64_t> cols;
   std::vector<double> vals;
-  std::vector<double> coords;  // [rows][2]
+  std::vector<double> coords;  // [rows][dims] (morton keys)
+  int dims = 2;
   int64_t output_size = 0;
   int64_t n_cols = 0;
   int64_t rows() const { return static_cast<int64_t>(row_ptr.size()) - 1; }
   int64_t nnz() const { return row_ptr.empty() ? 0 : row_ptr.back(); }
 };
 
-// Active-row transpose with grid-cell coordinates (transpose_sparse, :209-231).
+// Active-row transpose with grid-cell coordinates (transpose_sparse, :209-231). A 3D view
+// (dims 3, cells (q0 G + q1) G + q2) gets coordinates (q2, q1, q0).
 SparseView transpose_view(const SparseView& v, int64_t grid_size);
 
 struct PackTile {
@@ -47,6 +49,15 @@ std::vector<int64_t> row_order(const SparseView& v, int policy, int k_tile);
 // tiles themselves (as the reference does); search keeps illegal tiles.
 std::vector<PackTile> pack_view(const SparseView& v, int planner, int policy, int k_tile,
                                 uint64_t seed, int threads);
+// The tiles of row groups [g0, g1) of a row order, in group order (pack_view is row_order
+// followed by this over every group); lets large views be packed and compressed in batches.
+// With the optimized planner and fast_above > 0, a group whose column union is larger than
+// fast_above is packed the fast way (sorted union in K32 runs, split24): the optimized
+// search grows faster than linearly in the union, and the grid cells next to the centre of
+// a 3D radial trajectory have unions of tens of thousands of samples.
+std::vector<PackTile> pack_groups(const SparseView& v, const std::vector<int64_t>& order, int64_t g0,
+                                  int64_t g1, int planner, int k_tile, uint64_t seed, int threads,
+                                  int64_t fast_above);
 
 struct GroupedTiles {
   std::vector<uint32_t> group_offsets;

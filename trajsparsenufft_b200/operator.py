@@ -44,10 +44,11 @@ def _dev_ptr(t, dtype, shape, name):
 
 
 def plan_desc(im_size=256, grid_size=512, coils=8, width=6, planner="optimized", policy="morton",
-              seed=20260823, threads=0, reference_layout=False, device=None) -> PlanDesc:
+              seed=20260823, threads=0, reference_layout=False, device=None, dims=2) -> PlanDesc:
     d = PlanDesc()
     check(lib().tsn_plan_desc_default(C.byref(d)))
     d.im_size, d.grid_size, d.coils, d.kernel_width = im_size, grid_size, coils, width
+    d.dims = int(dims)
     d.planner, d.policy, d.seed, d.threads = _lib.PLANNER[planner], _lib.POLICY[policy], seed, threads
     d.flags = _lib.FLAG_REFERENCE_LAYOUT if reference_layout else 0
     if device is None:
@@ -73,20 +74,23 @@ class Plan:
         self.coils = info.coils
         self.width = info.kernel_width
         self.components = info.components
+        self.dims = info.dims if info.dims in (2, 3) else 2
         self.info = {
             "samples": info.samples, "im_size": info.im_size, "grid_size": info.grid_size, "coils": info.coils,
             "kernel_width": info.kernel_width, "components": info.components,
             "groups": list(info.groups), "tiles": list(info.tiles), "active_rows": list(info.active_rows),
             "nnz": list(info.nnz), "pack_bytes": list(info.pack_bytes), "workspace_bytes": info.workspace_bytes,
-            "plan_seconds": info.plan_seconds, "interp": info.interp,
+            "plan_seconds": info.plan_seconds, "interp": info.interp, "dims": self.dims,
         }
 
     # ---- construction ------------------------------------------------------------------
     @classmethod
     def from_trajectory(cls, trajectory, *, im_size=256, grid_size=512, coils=8, width=6, planner="optimized",
                         policy="morton", seed=20260823, threads=0, reference_layout=False, device=None) -> "Plan":
-        t = np.ascontiguousarray(np.asarray(trajectory, dtype=np.float32).reshape(-1, 2))
-        d = plan_desc(im_size, grid_size, coils, width, planner, policy, seed, threads, reference_layout, device)
+        traj = np.asarray(trajectory, dtype=np.float32)
+        dims = 3 if traj.ndim == 2 and traj.shape[1] == 3 else 2
+        t = np.ascontiguousarray(traj.reshape(-1, dims))
+        d = plan_desc(im_size, grid_size, coils, width, planner, policy, seed, threads, reference_layout, device, dims)
         h = C.c_void_p()
         check(lib().tsn_plan_create_from_trajectory(ptr(t, C.c_float), t.shape[0], C.byref(d), C.byref(h)))
         return cls(h)
@@ -117,16 +121,28 @@ class Plan:
             pass
 
     # ---- operators ------------------------------------------------------------------------
+    @property
+    def image_shape(self) -> tuple:
+        """[N, N] for image plans, [N, N, N] for volume plans."""
+        return (self.im_size,) * self.dims
+
+    @property
+    def maps_shape(self) -> tuple:
+        return (self.coils,) + self.image_shape
+
+    @property
+    def grid_cells(self) -> int:
+        return self.grid_size ** self.dims
+
     def _image_shape(self, smaps):
-        n = self.im_size
-        return (n, n) if smaps is not None else (self.coils, n, n)
+        return self.image_shape if smaps is not None else self.maps_shape
 
     def forward(self, x, smaps=None, out=None, stream=None):
         """y[C, M] = A x (unnormalized NUFFT of x*S_c, or of coil images when smaps is None)."""
         torch = _torch()
         cf = torch.complex64
         xp = _dev_ptr(x, cf, self._image_shape(smaps), "x")
-        sp = None if smaps is None else _dev_ptr(smaps, cf, (self.coils, self.im_size, self.im_size), "smaps")
+        sp = None if smaps is None else _dev_ptr(smaps, cf, self.maps_shape, "smaps")
         if out is None:
             out = torch.empty((self.coils, self.samples), dtype=cf, device=x.device)
         yp = _dev_ptr(out, cf, (self.coils, self.samples), "out")
@@ -138,7 +154,7 @@ class Plan:
         torch = _torch()
         cf = torch.complex64
         yp = _dev_ptr(y, cf, (self.coils, self.samples), "y")
-        sp = None if smaps is None else _dev_ptr(smaps, cf, (self.coils, self.im_size, self.im_size), "smaps")
+        sp = None if smaps is None else _dev_ptr(smaps, cf, self.maps_shape, "smaps")
         if out is None:
             out = torch.empty(self._image_shape(smaps), dtype=cf, device=y.device)
         xp = _dev_ptr(out, cf, self._image_shape(smaps), "out")
@@ -158,11 +174,11 @@ class Plan:
         cf = torch.complex64
         n = self.im_size
         yp = _dev_ptr(y, cf, (self.coils, self.samples), "y")
-        sp = _dev_ptr(smaps, cf, (self.coils, n, n), "smaps")
+        sp = _dev_ptr(smaps, cf, self.maps_shape, "smaps")
         dp = None if density is None else _dev_ptr(density, torch.float32, (self.samples,), "density")
         if out is None:
-            out = torch.empty((n, n), dtype=cf, device=y.device)
-        xp = _dev_ptr(out, cf, (n, n), "out")
+            out = torch.empty(self.image_shape, dtype=cf, device=y.device)
+        xp = _dev_ptr(out, cf, self.image_shape, "out")
         hist = np.zeros(iters + 1, dtype=np.float64) if sync else None
         st = CgStatus() if sync else None
         if reliable_update_direction not in ("restart", "beta"):
@@ -188,18 +204,22 @@ class Plan:
         """Mean milliseconds per launch of each CG-iteration stage (CUDA events)."""
         torch = _torch()
         yp = _dev_ptr(y, torch.complex64, (self.coils, self.samples), "y")
-        sp = _dev_ptr(smaps, torch.complex64, (self.coils, self.im_size, self.im_size), "smaps")
+        sp = _dev_ptr(smaps, torch.complex64, self.maps_shape, "smaps")
         out = np.zeros(len(_lib.STAGES), dtype=np.float64)
         check(lib().tsn_profile_stages(self._h, yp, sp, int(reps), ptr(out, C.c_double), _stream_handle(stream)))
-        return dict(zip(_lib.STAGES, out.tolist()))
+        stages = dict(zip(_lib.STAGES, out.tolist()))
+        if self.dims == 2:  # images have no middle-axis stages
+            stages.pop("fwd_mid")
+            stages.pop("inv_mid")
+        return stages
 
     def fft_forward_panel(self, x, smaps=None, stream=None):
         """Forward FFT endpoint: (panel [G*G, 4C] f16 in q1-major rows, panel scale)."""
         torch = _torch()
         xp = _dev_ptr(x, torch.complex64, self._image_shape(smaps), "x")
-        sp = None if smaps is None else _dev_ptr(smaps, torch.complex64, (self.coils, self.im_size, self.im_size),
+        sp = None if smaps is None else _dev_ptr(smaps, torch.complex64, self.maps_shape,
                                                  "smaps")
-        panel = torch.empty((self.grid_size ** 2, 4 * self.coils), dtype=torch.float16, device=x.device)
+        panel = torch.empty((self.grid_cells, 4 * self.coils), dtype=torch.float16, device=x.device)
         scale = C.c_float(0.0)
         check(lib().tsn_fft_forward_panel(self._h, xp, sp, C.c_void_p(panel.data_ptr()), C.byref(scale),
                                           _stream_handle(stream)))
@@ -208,8 +228,8 @@ class Plan:
     def fft_adjoint_image(self, grid, smaps=None, out=None, stream=None):
         """Adjoint FFT endpoint from a grid [G*G, C] c64 in q1-major rows."""
         torch = _torch()
-        gp = _dev_ptr(grid, torch.complex64, (self.grid_size ** 2, self.coils), "grid")
-        sp = None if smaps is None else _dev_ptr(smaps, torch.complex64, (self.coils, self.im_size, self.im_size),
+        gp = _dev_ptr(grid, torch.complex64, (self.grid_cells, self.coils), "grid")
+        sp = None if smaps is None else _dev_ptr(smaps, torch.complex64, self.maps_shape,
                                                  "smaps")
         if out is None:
             out = torch.empty(self._image_shape(smaps), dtype=torch.complex64, device=grid.device)
@@ -220,8 +240,8 @@ class Plan:
     def interp_component(self, view: str, component: int, dense_f16):
         """Raw out[rows,16] f32 = component(view) @ dense[n_cols,16] (reference.bin contract)."""
         torch = _torch()
-        rows = self.grid_size ** 2 if view == "G_T" else self.samples
-        cols = self.samples if view == "G_T" else self.grid_size ** 2
+        rows = self.grid_cells if view == "G_T" else self.samples
+        cols = self.samples if view == "G_T" else self.grid_cells
         dp = _dev_ptr(dense_f16, torch.float16, (cols, 16), "dense")
         out = torch.zeros((rows, 16), dtype=torch.float32, device=dense_f16.device)
         check(lib().tsn_interp_component(self._h, _lib.VIEW[view], int(component), dp, C.c_void_p(out.data_ptr()),
@@ -267,15 +287,15 @@ class Batch:
         if len(ys) != n_cases or len(smaps) != n_cases:
             raise ValueError("one y and one smaps per case")
         if outs is None:
-            outs = [torch.empty((pl.im_size, pl.im_size), dtype=cf, device=y.device) for pl, y in zip(self.plans, ys)]
+            outs = [torch.empty(pl.image_shape, dtype=cf, device=y.device) for pl, y in zip(self.plans, ys)]
         yp, sp, dp, xp = [], [], [], []
         for i, pl in enumerate(self.plans):
             n = pl.im_size
             yp.append(_dev_ptr(ys[i], cf, (pl.coils, pl.samples), f"ys[{i}]").value)
-            sp.append(_dev_ptr(smaps[i], cf, (pl.coils, n, n), f"smaps[{i}]").value)
+            sp.append(_dev_ptr(smaps[i], cf, pl.maps_shape, f"smaps[{i}]").value)
             w = None if densities is None else densities[i]
             dp.append(None if w is None else _dev_ptr(w, torch.float32, (pl.samples,), f"densities[{i}]").value)
-            xp.append(_dev_ptr(outs[i], cf, (n, n), f"outs[{i}]").value)
+            xp.append(_dev_ptr(outs[i], cf, pl.image_shape, f"outs[{i}]").value)
         arr = lambda v: (C.c_void_p * n_cases)(*v)
         st = (CgStatus * n_cases)() if sync else None
         rc = lib().tsn_batch_cg_sense(self._h, arr(yp), arr(sp), arr(dp), float(lam), float(operator_scale),

@@ -69,6 +69,26 @@ def kb_deapodization(im_size: int, grid_size: int, width: int) -> np.ndarray:
     return out
 
 
+def kb_weights_csr3(trajectory, im_size: int, grid_size: int, width: int):
+    """(row_ptr, cols, w) of the real KB weights of a [M, 3] trajectory (volume layout)."""
+    t = np.ascontiguousarray(np.asarray(trajectory, dtype=np.float32).reshape(-1, 3))
+    m = t.shape[0]
+    nnz = C.c_int64(0)
+    check(lib().tsn_kb_weights_csr3(ptr(t, C.c_float), m, im_size, grid_size, width, None, None, None, C.byref(nnz)))
+    row_ptr = np.zeros(m + 1, dtype=np.int64)
+    cols = np.zeros(nnz.value, dtype=np.int64)
+    w = np.zeros(nnz.value, dtype=np.float64)
+    check(lib().tsn_kb_weights_csr3(ptr(t, C.c_float), m, im_size, grid_size, width, ptr(row_ptr, C.c_int64),
+                                    ptr(cols, C.c_int64), ptr(w, C.c_double), C.byref(nnz)))
+    return row_ptr, cols, w
+
+
+def kb_deapodization3(im_size: int, grid_size: int, width: int) -> np.ndarray:
+    out = np.zeros((im_size,) * 3, dtype=np.float64)
+    check(lib().tsn_kb_deapodization3(im_size, grid_size, width, ptr(out, C.c_double)))
+    return out
+
+
 def _csr_args(row_ptr, cols, vals, row_ids, coords):
     row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
     cols = np.ascontiguousarray(cols, dtype=np.int64)

@@ -125,3 +125,70 @@ def uneven_batch(count: int = 48, seed: int = BASE_SEED) -> list[dict]:
             kind = f"spiral {inter}x{samples}"
         cases.append({"n": n, "g": 2 * n, "c": c, "trajectory": traj, "kind": kind, "seed": seed + i})
     return cases
+
+
+# ---- volumes (3D kooshball) -----------------------------------------------------------------
+def _grid3(n: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    coords = (np.arange(n, dtype=np.float64) - n // 2) / n
+    return np.meshgrid(coords, coords, coords, indexing="ij")
+
+
+def ellipsoid_phantom(n: int, seed: int, ellipsoids: int = 12) -> np.ndarray:
+    """[N, N, N] complex64 phantom: random ellipsoids (magnitudes U(0.1, 1), random
+    orientation) times a smooth linear-ramp phase."""
+    rng = np.random.default_rng(seed)
+    z, y, x = _grid3(n)
+    vol = np.zeros((n, n, n), dtype=np.float64)
+    for _ in range(ellipsoids):
+        centre = rng.uniform(-0.25, 0.25, size=3)
+        axes = rng.uniform(0.05, 0.3, size=3)
+        # random rotation from a QR of a Gaussian matrix (det fixed to +1)
+        q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+        q = q * np.sign(np.diag(r))[None, :]
+        if np.linalg.det(q) < 0:
+            q[:, 0] = -q[:, 0]
+        mag = rng.uniform(0.1, 1.0)
+        d = np.stack((z - centre[0], y - centre[1], x - centre[2]), axis=-1)
+        local = d @ q
+        inside = ((local / axes) ** 2).sum(axis=-1) <= 1.0
+        vol += mag * inside
+    slope = rng.uniform(-1.0, 1.0, size=3)
+    phase = np.exp(1j * math.pi * (slope[0] * z + slope[1] * y + slope[2] * x))
+    return (vol * phase).astype(np.complex64)
+
+
+def coil_maps3(n: int, coils: int, seed: int) -> np.ndarray:
+    """[C, N, N, N] complex64 Gaussian-blob sensitivities with centres spread on a sphere of
+    radius 0.7 FOV (Fibonacci lattice), sigma 0.4 FOV, random linear phase, RSS = 1."""
+    rng = np.random.default_rng(seed + 7919)
+    z, y, x = _grid3(n)
+    maps = np.zeros((coils, n, n, n), dtype=np.complex128)
+    golden = math.pi * (3.0 - math.sqrt(5.0))
+    for c in range(coils):
+        cz = 1.0 - 2.0 * (c + 0.5) / coils
+        ring = math.sqrt(max(0.0, 1.0 - cz * cz))
+        centre = 0.7 * np.array([cz, ring * math.sin(golden * c), ring * math.cos(golden * c)])
+        blob = np.exp(-((z - centre[0]) ** 2 + (y - centre[1]) ** 2 + (x - centre[2]) ** 2) / (2.0 * 0.4 ** 2))
+        slope = rng.uniform(-1.0, 1.0, size=3)
+        maps[c] = blob * np.exp(1j * math.pi * (slope[0] * z + slope[1] * y + slope[2] * x))
+    rss = np.sqrt(np.sum(np.abs(maps) ** 2, axis=0))
+    return (maps / rss).astype(np.complex64)
+
+
+# 3D golden means for radial sampling (Chan et al., MRM 2009): phi2 is the real root of
+# x^3 + x - 1 = 0 and phi1 = phi2^2
+GOLDEN_MEANS_3D = (0.465571231876768, 0.682327803828019)
+
+
+def kooshball(spokes: int, readout: int) -> np.ndarray:
+    """[spokes*readout, 3] float32 golden-means 3D radial trajectory (cycles/pixel): spoke m
+    has direction cos(polar) = 2 frac(m phi1) - 1, azimuth 2 pi frac(m phi2), and samples
+    linspace(-0.5, 0.5, readout, endpoint=False) along it."""
+    m = np.arange(spokes, dtype=np.float64)
+    kz = 2.0 * np.mod(m * GOLDEN_MEANS_3D[0], 1.0) - 1.0
+    az = 2.0 * math.pi * np.mod(m * GOLDEN_MEANS_3D[1], 1.0)
+    ring = np.sqrt(np.maximum(0.0, 1.0 - kz * kz))
+    direction = np.stack((kz, ring * np.sin(az), ring * np.cos(az)), axis=-1)  # [spokes, 3]
+    radius = np.linspace(-0.5, 0.5, readout, endpoint=False, dtype=np.float64)
+    traj = direction[:, None, :] * radius[None, :, None]
+    return traj.reshape(-1, 3).astype(np.float32)
