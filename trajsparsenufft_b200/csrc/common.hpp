@@ -2,10 +2,13 @@
 // random.Random generator the reference planner is defined with.
 #pragma once
 
+#include <sys/mman.h>
+
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/trajsparsenufft.h"
 
@@ -20,6 +23,22 @@ struct Error : std::runtime_error {
 [[noreturn]] inline void fail(tsn_status s, const std::string& what) { throw Error(s, what); }
 
 void set_last_error(const std::string& text);
+
+// Size a large host vector to n elements, asking the kernel for transparent huge pages before
+// the first touch (multi-GB planner arrays otherwise fault in 4 KB at a time, which costs
+// minutes of system time on virtualized hosts). Advisory: without THP it is a plain resize.
+template <class T>
+void resize_huge(std::vector<T>& v, size_t n) {
+  if (n * sizeof(T) >= (size_t(64) << 20) && v.capacity() < n) {
+    std::vector<T>().swap(v);
+    v.reserve(n);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(v.data());
+    const uintptr_t lo = (a + 0x1FFFFF) & ~uintptr_t(0x1FFFFF);
+    const uintptr_t hi = (a + n * sizeof(T)) & ~uintptr_t(0x1FFFFF);
+    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);
+  }
+  v.resize(n);
+}
 
 // Round an IEEE binary64 value to binary16, round-to-nearest-even, directly from the
 // double bits (numpy's float64 -> float16 cast, used by compress_tile at

@@ -194,7 +194,8 @@ KbCsr kb_weights_csr3(const float* traj, int64_t m, int im_size, int grid_size, 
     if (!std::isfinite(traj[i])) fail(TSN_ERR_NONFINITE, "trajectory contains non-finite coordinates");
   if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
   KbCsr out;
-  out.row_ptr.assign(static_cast<size_t>(m) + 1, 0);
+  resize_huge(out.row_ptr, static_cast<size_t>(m) + 1);
+  out.row_ptr[0] = 0;
   auto axes = [&](int64_t r, Axis (&ax)[3]) {
     for (int d = 0; d < 3; ++d) axis_weights(static_cast<double>(traj[3 * r + d]) * grid_size, width, g, beta, i0b, ax[d]);
   };
@@ -208,8 +209,8 @@ KbCsr kb_weights_csr3(const float* traj, int64_t m, int im_size, int grid_size, 
     out.row_ptr[r + 1] = n[0] * n[1] * n[2];
   });
   for (int64_t r = 0; r < m; ++r) out.row_ptr[r + 1] += out.row_ptr[r];
-  out.cols.resize(static_cast<size_t>(out.row_ptr[m]));
-  out.re.resize(out.cols.size());
+  resize_huge(out.cols, static_cast<size_t>(out.row_ptr[m]));
+  resize_huge(out.re, out.cols.size());
   // pass 2: entries, sorted by cell
   parallel_rows(m, threads, [&](int64_t r) {
     Axis ax[3];

@@ -57,71 +57,108 @@ static void parallel_for(int64_t n, int threads, F&& body) {
   if (err) std::rethrow_exception(err);
 }
 
-// Volume transpose on all host cores: atomic cell counts, an atomic scatter, then each row's
-// entries sorted by source row, which gives exactly the serial transpose's layout (a
-// sample touches a cell at most once).
+// Volume transpose on all host cores without a random scatter over the whole matrix: entries
+// are streamed into buckets of 2^14 consecutive cells (each thread owns a contiguous run of
+// source rows, so a bucket holds every cell's entries in ascending source-row order), then
+// each bucket is counting-sorted by cell into its contiguous output range. The layout is
+// exactly the serial transpose's.
 static SparseView transpose_view_parallel(const SparseView& v, int64_t grid_size) {
   const int threads = resolve_threads(0);
-  const int64_t n_rows = v.rows();
-  const int64_t blocks = (n_rows + 4095) / 4096;
-  std::unique_ptr<std::atomic<int32_t>[]> count(new std::atomic<int32_t>[v.n_cols]);
-  for (int64_t c = 0; c < v.n_cols; ++c) count[c].store(0, std::memory_order_relaxed);
+  const int64_t n_rows = v.rows(), nnz = v.nnz(), n_cols = v.n_cols;
+  constexpr int kBucketShift = 14;
+  const int64_t buckets = (n_cols + (int64_t(1) << kBucketShift) - 1) >> kBucketShift;
+  if (n_cols > (int64_t(1) << 31) || n_rows > (int64_t(1) << 31)) fail(TSN_ERR_UNSUPPORTED, "view too large");
+  for (int64_t k = 0; k < nnz; k += std::max<int64_t>(1, nnz / 4096))
+    if (v.cols[k] < 0 || v.cols[k] >= n_cols) fail(TSN_ERR_SHAPE, "column id out of range");
+  // pass 1: per-thread bucket histograms over contiguous source-row runs
+  const int T = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(threads, n_rows)));
+  std::vector<int64_t> hist(static_cast<size_t>(T) * buckets, 0);
   std::atomic<bool> bad{false};
-  parallel_for(blocks, threads, [&](int64_t b) {
-    const int64_t r1 = std::min(n_rows, (b + 1) * 4096);
-    for (int64_t k = v.row_ptr[b * 4096]; k < v.row_ptr[r1]; ++k) {
+  auto row_run = [&](int th, int64_t& r0, int64_t& r1) {
+    r0 = n_rows * th / T;
+    r1 = n_rows * (th + 1) / T;
+  };
+  parallel_for(T, T, [&](int64_t th) {
+    int64_t r0, r1;
+    row_run(static_cast<int>(th), r0, r1);
+    int64_t* h = &hist[static_cast<size_t>(th) * buckets];
+    for (int64_t k = v.row_ptr[r0]; k < v.row_ptr[r1]; ++k) {
       const int64_t c = v.cols[k];
-      if (c < 0 || c >= v.n_cols) {
+      if (c < 0 || c >= n_cols) {
         bad.store(true);
         return;
       }
-      count[c].fetch_add(1, std::memory_order_relaxed);
+      ++h[c >> kBucketShift];
     }
   });
   if (bad.load()) fail(TSN_ERR_SHAPE, "column id out of range");
+  // write offsets: bucket-major, thread order within a bucket
+  std::vector<int64_t> bucket_start(buckets + 1, 0);
+  std::vector<int64_t> off(static_cast<size_t>(T) * buckets);
+  int64_t pos = 0;
+  for (int64_t b = 0; b < buckets; ++b) {
+    bucket_start[b] = pos;
+    for (int th = 0; th < T; ++th) {
+      off[static_cast<size_t>(th) * buckets + b] = pos;
+      pos += hist[static_cast<size_t>(th) * buckets + b];
+    }
+  }
+  bucket_start[buckets] = pos;
+  hist.clear();
+  hist.shrink_to_fit();
+  struct Entry {
+    int32_t cell, row;
+    double val;
+  };
+  std::vector<Entry> staged;
+  resize_huge(staged, static_cast<size_t>(nnz));
+  parallel_for(T, T, [&](int64_t th) {
+    int64_t r0, r1;
+    row_run(static_cast<int>(th), r0, r1);
+    int64_t* o = &off[static_cast<size_t>(th) * buckets];
+    for (int64_t r = r0; r < r1; ++r) {
+      const int32_t logical = static_cast<int32_t>(v.row_ids[r]);
+      for (int64_t k = v.row_ptr[r]; k < v.row_ptr[r + 1]; ++k) {
+        const int64_t c = v.cols[k];
+        staged[o[c >> kBucketShift]++] = Entry{static_cast<int32_t>(c), logical, v.vals[k]};
+      }
+    }
+  });
+  off.clear();
+  off.shrink_to_fit();
+  // pass 2: per-bucket cell counts, then the global row structure
+  std::vector<int32_t> count;
+  resize_huge(count, static_cast<size_t>(n_cols));
+  parallel_for(buckets, threads, [&](int64_t b) {
+    for (int64_t k = bucket_start[b]; k < bucket_start[b + 1]; ++k) ++count[staged[k].cell];
+  });
   SparseView t;
-  t.output_size = v.n_cols;
+  t.output_size = n_cols;
   t.n_cols = v.output_size;
   t.dims = v.dims;
-  std::unique_ptr<std::atomic<int64_t>[]> cursor(new std::atomic<int64_t>[v.n_cols]);
   t.row_ptr.push_back(0);
-  for (int64_t c = 0; c < v.n_cols; ++c) {
-    const int32_t n = count[c].load(std::memory_order_relaxed);
-    cursor[c].store(t.row_ptr.back(), std::memory_order_relaxed);
-    if (!n) continue;
+  std::vector<int64_t> row_start;
+  resize_huge(row_start, static_cast<size_t>(n_cols));
+  for (int64_t c = 0; c < n_cols; ++c) {
+    row_start[c] = t.row_ptr.back();
+    if (!count[c]) continue;
     t.row_ids.push_back(c);
     t.coords.push_back(static_cast<double>(c % grid_size));
     t.coords.push_back(static_cast<double>((c / grid_size) % grid_size));
     t.coords.push_back(static_cast<double>(c / (grid_size * grid_size)));
-    t.row_ptr.push_back(t.row_ptr.back() + n);
+    t.row_ptr.push_back(t.row_ptr.back() + count[c]);
   }
-  count.reset();
-  t.cols.resize(v.nnz());
-  t.vals.resize(v.nnz());
-  parallel_for(blocks, threads, [&](int64_t b) {
-    const int64_t r0 = b * 4096, r1 = std::min(n_rows, r0 + 4096);
-    for (int64_t r = r0; r < r1; ++r) {
-      const int64_t logical = v.row_ids[r];
-      for (int64_t k = v.row_ptr[r]; k < v.row_ptr[r + 1]; ++k) {
-        const int64_t at = cursor[v.cols[k]].fetch_add(1, std::memory_order_relaxed);
-        t.cols[at] = logical;
-        t.vals[at] = v.vals[k];
-      }
-    }
-  });
-  cursor.reset();
-  const int64_t out_rows = t.rows();
-  parallel_for((out_rows + 1023) / 1024, threads, [&](int64_t b) {
-    std::vector<std::pair<int64_t, double>> tmp;
-    for (int64_t r = b * 1024; r < std::min(out_rows, (b + 1) * 1024); ++r) {
-      const int64_t a = t.row_ptr[r], e = t.row_ptr[r + 1];
-      tmp.clear();
-      for (int64_t k = a; k < e; ++k) tmp.emplace_back(t.cols[k], t.vals[k]);
-      std::sort(tmp.begin(), tmp.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
-      for (int64_t k = a; k < e; ++k) {
-        t.cols[k] = tmp[k - a].first;
-        t.vals[k] = tmp[k - a].second;
-      }
+  count.clear();
+  count.shrink_to_fit();
+  resize_huge(t.cols, static_cast<size_t>(nnz));
+  resize_huge(t.vals, static_cast<size_t>(nnz));
+  // pass 3: stable scatter of each bucket into its contiguous output range
+  parallel_for(buckets, threads, [&](int64_t b) {
+    for (int64_t k = bucket_start[b]; k < bucket_start[b + 1]; ++k) {
+      const Entry& e = staged[k];
+      const int64_t at = row_start[e.cell]++;
+      t.cols[at] = e.row;
+      t.vals[at] = e.val;
     }
   });
   return t;
