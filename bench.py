@@ -47,6 +47,7 @@ CONFIGS = {
     "grad4": dict(grad=True, cases=4, n=256, g=512, c=8, spokes=128, readout=512, width=6, iters=10, checkpoint=2,
                   density=False),
     "kooshball": dict(volume=True, n=128, g=256, c=8, spokes=16384, readout=256, width=4, iters=10),
+    "vol64": dict(volume=True, n=64, g=128, c=8, spokes=2048, readout=128, width=4, iters=10),
 }
 VOLUME_METRIC = "CG-SENSE recons/s 128^3x8coil x10CG, 3D golden-means kooshball"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
@@ -593,38 +594,93 @@ def run_grad(args, cfg) -> dict | None:
         torch.cuda.synchronize()
         return max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(st, en)), dev)
 
-    with ClockSampler(local) as clocks:
-        grad_ms = timed(grad_step)
-    fwd_ms = timed(fwd_step)
+    eager_grad_ms = timed(grad_step)
+    eager_fwd_ms = timed(fwd_step)
     plain_ms = timed(plain_step)
 
-    # end to end: inputs from pinned host memory, loss and all gradients back to the host
+    # The whole gradient step (all cases' forward solves, the loss and the backward) as one
+    # CUDA graph: static input tensors, leaves made once, grads allocated at capture and
+    # overwritten by every replay.
+    y_st = [y.clone() for y in ys]
+    s_st = [s.clone() for s in maps]
+    yl = [y.detach().requires_grad_(True) for y in y_st]
+    sl = [s.detach().requires_grad_(True) for s in s_st]
+    x0l = [torch.zeros((n, n), dtype=torch.complex64, device=dev, requires_grad=True) for _ in ys]
+    leaves = yl + sl + x0l
+
+    def graph_body():
+        loss = 0.0
+        for y, s, x0, xt in zip(yl, sl, x0l, xts):
+            xk = tad.cg_sense(y, s, ops, x0=x0, x0_zero=True, lam=lam, iters=iters, checkpoint=every)
+            loss = loss + (xk - xt).abs().pow(2).sum()
+        loss.backward()
+        return loss
+
+    def fwd_body():
+        with torch.no_grad():
+            return [tad.cg_sense(y, s, ops, lam=lam, iters=iters, checkpoint=every) for y, s in zip(y_st, s_st)]
+
+    def capture(body, clear_grads):
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(3):
+                if clear_grads:
+                    for leaf in leaves:
+                        leaf.grad = None
+                body()
+        torch.cuda.current_stream().wait_stream(side)
+        if clear_grads:
+            for leaf in leaves:
+                leaf.grad = None
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+            result = body()
+        return graph, result
+
+    g_grad, g_loss = capture(graph_body, True)
+    g_fwd, _ = capture(fwd_body, False)
+    # the graph replays the eager step's kernels: its gradients match an eager step's
+    g_grad.replay()
+    loss_e, leaves_e = grad_step()
+    torch.cuda.synchronize()
+    eager_leaves = [trip[k] for k in range(3) for trip in leaves_e]  # all y, all maps, all x0: as `leaves`
+    graph_vs_eager = max(
+        float(torch.linalg.vector_norm(a.grad - b.grad) / torch.linalg.vector_norm(b.grad).clamp_min(1e-30))
+        for a, b in zip(leaves, eager_leaves))
+    with ClockSampler(local) as clocks:
+        grad_ms = timed(g_grad.replay)
+    fwd_ms = timed(g_fwd.replay)
+
+    # end to end: inputs from pinned host memory into the graph's static inputs, then the loss
+    # and every gradient back to the host
     y_h = [y.cpu().pin_memory() for y in ys]
     s_h = [s.cpu().pin_memory() for s in maps]
+    grads_h = [torch.empty(leaf.shape, dtype=leaf.dtype).pin_memory() for leaf in leaves]
+    loss_h = torch.empty((), dtype=g_loss.dtype).pin_memory()
 
     def e2e_step():
-        y_d = [h.to(dev, non_blocking=True) for h in y_h]
-        s_d = [h.to(dev, non_blocking=True) for h in s_h]
-        loss, leaves = grad_step(y_d, s_d)
-        host = [loss.detach().to("cpu", non_blocking=True)]
-        for yl, sl, x0 in leaves:
-            host += [yl.grad.to("cpu", non_blocking=True), sl.grad.to("cpu", non_blocking=True),
-                     x0.grad.to("cpu", non_blocking=True)]
-        return host
+        for dst, h in zip(y_st + s_st, y_h + s_h):
+            dst.copy_(h, non_blocking=True)
+        g_grad.replay()
+        loss_h.copy_(g_loss.detach(), non_blocking=True)
+        for h, leaf in zip(grads_h, leaves):
+            h.copy_(leaf.grad, non_blocking=True)
+
+    def e2e_run(nsteps):
+        es = [torch.cuda.Event(enable_timing=True) for _ in range(nsteps)]
+        ee = [torch.cuda.Event(enable_timing=True) for _ in range(nsteps)]
+        for k in range(nsteps):
+            flush.zero_()
+            es[k].record()
+            e2e_step()
+            ee[k].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in zip(es, ee)), None
 
     e2e_steps = max(3, args.steps // 2)
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    es = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
-    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
-    for k in range(e2e_steps):
-        flush.zero_()
-        es[k].record()
-        e2e_step()
-        ee[k].record()
-    torch.cuda.synchronize()
-    e2e_max_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(es, ee)), dev)
+    e2e_run(2)
+    e2e_ms, _, e2e_repeats = median_run(lambda: e2e_run(e2e_steps), dev)
     if world > 1:
         torch.distributed.destroy_process_group()
     cases = cfg["cases"]
@@ -639,17 +695,24 @@ def run_grad(args, cfg) -> dict | None:
                                f"CG-SENSE iterations (checkpoint every {every}); loss |x - x_true|^2, gradients "
                                "w.r.t. k-space data, coil maps and x0",
                    "recons_per_step": cases, "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "step": "one CUDA graph per step: forward solves, loss and backward of all cases"},
         "forward_only": {"value": round(job_rate(world, cases, args.steps, fwd_ms), 3), "unit": "recons/s",
                          "ms_per_step": round(fwd_ms / args.steps, 4)},
         "backward_over_forward": round((grad_ms - fwd_ms) / fwd_ms, 3),
+        "graph_grads_rel_diff_vs_eager": graph_vs_eager,
+        "eager": {"value": round(job_rate(world, cases, args.steps, eager_grad_ms), 3),
+                  "ms_per_step": round(eager_grad_ms / args.steps, 4),
+                  "forward_only_ms_per_step": round(eager_fwd_ms / args.steps, 4),
+                  "backward_over_forward": round((eager_grad_ms - eager_fwd_ms) / eager_fwd_ms, 3)},
         "plain_graph_solver": {"value": round(job_rate(world, cases, args.steps, plain_ms), 3),
                                "unit": "recons/s", "ms_per_step": round(plain_ms / args.steps, 4)},
-        "e2e": {"value": round(job_rate(world, cases, e2e_steps, e2e_max_ms), 3),
+        "e2e": {"value": round(job_rate(world, cases, e2e_steps, e2e_ms), 3),
                 "unit": "recons/s (with gradients)",
                 "h2d_bytes_per_step": int(sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)),
-                "d2h_bytes_per_step": int(8 + sum(y.numel() * 8 for y in ys) + sum(s.numel() * 8 for s in maps)
-                                          + cases * n * n * 8)},
+                "d2h_bytes_per_step": int(8 + sum(leaf.numel() * 8 for leaf in leaves)),
+                "repeats": [round(job_rate(world, cases, e2e_steps, v), 3) for v in e2e_repeats],
+                "statistic": f"median of {len(e2e_repeats)} runs of {e2e_steps} steps"},
         "gpu_launches": None,
         "clocks": clocks.summary(),
     }
@@ -836,7 +899,7 @@ def run_volume(args, cfg) -> dict | None:
     recon_bytes = iters * sum(alg.values())
     m = plan.samples
     out = {
-        "metric": VOLUME_METRIC, "value": round(value, 4), "unit": "recons/s", "n_gpus": world, "steps": args.steps,
+        "metric": VOLUME_METRIC if cfg["n"] == 128 else VOLUME_METRIC.replace("128^3", f"{n}^3"), "value": round(value, 4), "unit": "recons/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f16x2->f32 (f64 CG scalars)", "data": "synthetic",
         "config": {"workload": f"{n}^3 volume, {g}^3 grid, {c} coils, golden-means kooshball {cfg['spokes']}x"

@@ -99,3 +99,58 @@ def test_differentiable_forward_matches_graph_solver():
         x_diff = tad.cg_sense(yt, st, tad.PlanOps(plan), lam=LAM, iters=ITERS)
     rel = float((x_diff - x_graph).abs().norm() / x_graph.abs().norm())
     assert rel <= 1e-4
+
+
+def test_graph_captured_gradient_step_matches_eager():
+    """The whole differentiable step (forward solve, loss, backward) captured as one CUDA graph
+    gives the eager step's gradients; replays with new inputs in the static tensors follow them."""
+    from trajsparsenufft_b200 import autograd as tad
+    from trajsparsenufft_b200.operator import Plan
+    traj, x, s, n, g, c, j, _ = case("small")
+    plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=j)
+    ops = tad.PlanOps(plan)
+    y0 = torch.from_numpy(measurement("small")).cuda()
+    s0 = torch.from_numpy(s).cuda()
+    xt = torch.from_numpy(x).cuda()
+
+    def eager(y, smaps):
+        yl = y.detach().clone().requires_grad_(True)
+        sl = smaps.detach().clone().requires_grad_(True)
+        x0 = torch.zeros((n, n), dtype=torch.complex64, device="cuda", requires_grad=True)
+        loss = (tad.cg_sense(yl, sl, ops, x0=x0, lam=LAM, iters=ITERS, checkpoint=2) - xt).abs().pow(2).sum()
+        loss.backward()
+        return loss.detach(), [yl.grad, sl.grad, x0.grad]
+
+    y_st, s_st = y0.clone(), s0.clone()
+    leaves = [y_st.detach().requires_grad_(True), s_st.detach().requires_grad_(True),
+              torch.zeros((n, n), dtype=torch.complex64, device="cuda", requires_grad=True)]
+
+    def body():
+        yl, sl, x0 = leaves
+        loss = (tad.cg_sense(yl, sl, ops, x0=x0, x0_zero=True, lam=LAM, iters=ITERS, checkpoint=2)
+                - xt).abs().pow(2).sum()
+        loss.backward()
+        return loss
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            for leaf in leaves:
+                leaf.grad = None
+            body()
+    torch.cuda.current_stream().wait_stream(side)
+    for leaf in leaves:
+        leaf.grad = None
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+        loss_g = body()
+    for scale in (1.0, 0.5):
+        y_st.copy_(y0 * scale)
+        graph.replay()
+        loss_e, grads_e = eager(y0 * scale, s0)
+        torch.cuda.synchronize()
+        assert torch.allclose(loss_g, loss_e, rtol=1e-6, atol=0)
+        for leaf, ge in zip(leaves, grads_e):
+            rel = float(torch.linalg.vector_norm(leaf.grad - ge) / torch.linalg.vector_norm(ge))
+            assert rel <= 1e-6, rel

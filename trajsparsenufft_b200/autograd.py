@@ -19,8 +19,10 @@ reference_sparse_solver.py cg_sense) from an initial image x0:
     q = M p, alpha = rho / Re<p, q>, x += alpha p, r -= alpha q, beta = rho'/rho, p = r + beta p.
 Backward runs the adjoint recurrences of these steps in reverse, restarting each segment from
 a checkpoint (x, r, p, rho) stored every `checkpoint` iterations, and returns gradients for
-the k-space data y, the coil maps and x0.  Each reverse step applies G twice per coil (the
-recomputed forward step and the adjoint of q = M p, which also yields the coil-map term).
+the k-space data y, the coil maps and x0.  A checkpoint also keeps q = M p of its own step
+(and the coil images G(S p) when the maps need gradients), which the forward computed anyway,
+so a segment recomputes `checkpoint - 1` forward steps.  Each reverse step applies G once per
+coil for the adjoint of q = M p, which also yields the coil-map term.
 """
 
 from __future__ import annotations
@@ -118,18 +120,25 @@ class UnrolledCgSense(torch.autograd.Function):
     """x_K of `iters` CG-SENSE iterations from x0; differentiable in y, smaps and x0."""
 
     @staticmethod
-    def forward(ctx, y, smaps, x0, density, ops, lam, iters, checkpoint):
+    def forward(ctx, y, smaps, x0, density, ops, lam, iters, checkpoint, x0_zero):
         S = _Sense(ops, smaps, density, lam)
         u = ops.adjoint_coils(S.weigh(y))          # F^H W y, coil images
         b = S.combine(u)
-        x0_zero = not bool(x0.abs().amax() > 0)
+        if x0_zero is None:                        # decided from the values (a host sync)
+            x0_zero = not bool(x0.abs().amax() > 0)
         x = x0.clone()
         r = b.clone() if x0_zero else b - S.M(x0)
         p = r.clone()
         rho = _rdot(r, r)
         cps = [(x, r, p, rho)]
-        for k in range(iters):
-            q = S.M(p)
+        need_s = ctx.needs_input_grad[1]
+        firsts = []   # q = M p (and the coil images G(S p) when maps need gradients) of each
+        for k in range(iters):   # checkpointed step: the backward reuses them instead of recomputing
+            if k % checkpoint == 0:
+                q, t = S.M_coils(p)
+                firsts.append((q, t) if need_s else (q,))
+            else:
+                q = S.M(p)
             alpha = rho / _rdot(p, q)
             x = x + alpha * p
             r = r - alpha * q
@@ -140,7 +149,8 @@ class UnrolledCgSense(torch.autograd.Function):
                 cps.append((x, r, p, rho))
         ctx.ops, ctx.lam, ctx.iters, ctx.checkpoint, ctx.x0_zero = ops, lam, iters, checkpoint, x0_zero
         ctx.has_density = density is not None
-        flat = [t for cp in cps for t in cp]
+        ctx.first_width = 2 if need_s else 1
+        flat = [v for cp in cps for v in cp] + [v for f in firsts for v in f]
         ctx.save_for_backward(smaps, x0, u, *(() if density is None else (density,)), *flat)
         return x
 
@@ -150,7 +160,11 @@ class UnrolledCgSense(torch.autograd.Function):
         smaps, x0, u = saved[0], saved[1], saved[2]
         density = saved[3] if ctx.has_density else None
         flat = saved[4 if ctx.has_density else 3:]
-        cps = [tuple(flat[i:i + 4]) for i in range(0, len(flat), 4)]
+        n_seg = (ctx.iters + ctx.checkpoint - 1) // ctx.checkpoint   # segments (firsts)
+        n_cp = max(1, n_seg)                                          # checkpoints incl. the start
+        cps = [tuple(flat[i:i + 4]) for i in range(0, 4 * n_cp, 4)]
+        fw = ctx.first_width
+        firsts = [tuple(flat[4 * n_cp + i:4 * n_cp + i + fw]) for i in range(0, fw * n_seg, fw)]
         S = _Sense(ctx.ops, smaps, density, ctx.lam)
         need_y, need_s, need_x0 = ctx.needs_input_grad[0], ctx.needs_input_grad[1], ctx.needs_input_grad[2]
         c, iters = ctx.checkpoint, ctx.iters
@@ -163,8 +177,10 @@ class UnrolledCgSense(torch.autograd.Function):
             k0, k1 = seg * c, min(seg * c + c, iters)
             _, r, p, rho = cps[seg]
             steps = []
-            for _k in range(k0, k1):  # recompute this segment's forward states
-                if need_s:
+            for k in range(k0, k1):  # recompute this segment's forward states
+                if k == k0:          # kept by the forward with the checkpoint
+                    q, t = firsts[seg][0], (firsts[seg][1] if need_s else None)
+                elif need_s:
                     q, t = S.M_coils(p)
                 else:
                     q, t = S.M(p), None
@@ -212,14 +228,20 @@ class UnrolledCgSense(torch.autograd.Function):
             gs = sb
         if need_y:
             gy = S.weigh(ctx.ops.forward_coils(smaps * rb))
-        return gy, gs, gx0, None, None, None, None, None
+        return gy, gs, gx0, None, None, None, None, None, None
 
 
-def cg_sense(y, smaps, ops, *, x0=None, density=None, lam=1e-4, iters=10, checkpoint=2):
+def cg_sense(y, smaps, ops, *, x0=None, density=None, lam=1e-4, iters=10, checkpoint=2, x0_zero=None):
     """Differentiable unrolled CG-SENSE: x after `iters` iterations of (A^H W A + lam) x = A^H W y
-    from x0 (zero by default), with CG states checkpointed every `checkpoint` iterations."""
+    from x0 (zero by default), with CG states checkpointed every `checkpoint` iterations.
+
+    x0_zero states whether x0 is all zeros (which saves one operator application); None
+    decides it from x0's values, a device-to-host read that a CUDA-graph capture of the step
+    cannot contain, so graph-captured steps pass it explicitly."""
     if x0 is None:
         x0 = torch.zeros(smaps.shape[1:], dtype=smaps.dtype, device=smaps.device)
+        x0_zero = True
     if checkpoint < 1:
         raise ValueError("checkpoint interval must be >= 1")
-    return UnrolledCgSense.apply(y, smaps, x0, density, ops, float(lam), int(iters), int(checkpoint))
+    return UnrolledCgSense.apply(y, smaps, x0, density, ops, float(lam), int(iters), int(checkpoint),
+                                 None if x0_zero is None else bool(x0_zero))
