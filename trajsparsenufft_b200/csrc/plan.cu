@@ -175,24 +175,41 @@ uint32_t live_columns(const HostView& h, int64_t t) {
   return m;
 }
 
-// Persistent-warp runs: contiguous item runs of about tiles / warps tiles each. Run w ends at
-// the item boundary nearest to (w + 1) * tiles / warps, so no run drifts by more than half an
-// item from the ideal split.
+// Persistent-warp runs: contiguous item runs with the smallest possible longest run. A binary
+// search finds the least T for which a greedy fill (each run takes items while it stays at or
+// under T tiles) needs at most `warps` runs; the runs are that fill. Items are never split, so
+// T >= the longest item.
 std::vector<int2> cut_ranges(const std::vector<int64_t>& item_ends, int64_t tiles, int warps) {
   warps = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(warps, static_cast<int64_t>(item_ends.size()))));
-  std::vector<int2> ranges;
-  int64_t run_start = 0;
-  size_t i = 0;
-  for (int w = 0; w < warps && run_start < tiles; ++w) {
-    const double ideal = static_cast<double>(tiles) * (w + 1) / warps;
-    while (i + 1 < item_ends.size() && item_ends[i] <= run_start) ++i;  // first boundary after the start
-    while (i + 1 < item_ends.size() &&
-           std::abs(static_cast<double>(item_ends[i + 1]) - ideal) <= std::abs(static_cast<double>(item_ends[i]) - ideal))
-      ++i;
-    const int64_t end = (w + 1 == warps) ? tiles : item_ends[i];
-    ranges.push_back(make_int2(static_cast<int>(run_start), static_cast<int>(end)));
-    run_start = end;
+  auto fill = [&](int64_t cap, std::vector<int2>* out) {
+    int64_t runs = 0, start = 0, prev = 0;
+    for (size_t i = 0; i < item_ends.size(); ++i) {
+      if (item_ends[i] - start > cap) {  // item i starts a new run
+        if (out) out->push_back(make_int2(static_cast<int>(start), static_cast<int>(prev)));
+        ++runs;
+        start = prev;
+      }
+      prev = item_ends[i];
+    }
+    if (prev > start) {
+      if (out) out->push_back(make_int2(static_cast<int>(start), static_cast<int>(prev)));
+      ++runs;
+    }
+    return runs;
+  };
+  int64_t longest = 0, prev = 0;
+  for (int64_t e : item_ends) {
+    longest = std::max(longest, e - prev);
+    prev = e;
   }
+  int64_t lo = std::max<int64_t>(longest, (tiles + warps - 1) / warps), hi = std::max<int64_t>(lo, tiles);
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (fill(mid, nullptr) <= warps) hi = mid;
+    else lo = mid + 1;
+  }
+  std::vector<int2> ranges;
+  fill(lo, &ranges);
   return ranges;
 }
 
@@ -227,7 +244,29 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
     slots += nch;
     ++nsplit;
   }
-  items.insert(items.end(), small.begin(), small.end());
+  // stream order: each chunk of a split group (the long poles, first in their run) is followed
+  // by whole small groups up to the average run length, so runs can be cut close to the
+  // average instead of at multiples of the chunk length
+  {
+    int64_t total = 0;
+    for (const Item& it : items) total += it.t1 - it.t0;
+    for (const Item& it : small) total += it.t1 - it.t0;
+    const int warps_full = interp_resident_warps(4 * P->C, ncomp);
+    const double avg = static_cast<double>(total) / std::max(1, warps_full);
+    std::vector<Item> order;
+    order.reserve(items.size() + small.size());
+    size_t si = 0;
+    for (const Item& chunk : items) {
+      order.push_back(chunk);
+      double run = chunk.t1 - chunk.t0;
+      while (si < small.size() && run + 0.5 * (small[si].t1 - small[si].t0) <= avg) {
+        run += small[si].t1 - small[si].t0;
+        order.push_back(small[si++]);
+      }
+    }
+    order.insert(order.end(), small.begin() + static_cast<std::ptrdiff_t>(si), small.end());
+    items.swap(order);
+  }
   // persistent warps: contiguous runs of items with about the same number of tiles each;
   // records are stored in that stream order so each warp reads one contiguous range
   std::vector<uint8_t> records(static_cast<size_t>(tiles) * rec, 0);
