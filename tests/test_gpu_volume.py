@@ -17,6 +17,7 @@ from gpu_cases import rel_l2, volume_case, volume_measurement
 from oracle import kb as okb
 from oracle import nudft as onudft
 from oracle import operator as oop
+from trajsparsenufft_b200 import synth
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -124,3 +125,42 @@ def test_volume_and_image_in_one_batch_match_single_solves():
     outs, statuses = batch.cg_sense([yv, y2], [sv, st2], lam=1e-4, iters=6)
     assert all(s_["finite"] and s_["positive_curvature"] for s_ in statuses)
     assert torch.equal(outs[0], single_v) and torch.equal(outs[1], single_i)
+
+
+def test_volume_density_and_reliable_update():
+    """Density-weighted CG and the reliable-update CG (restart every 4 iterations) on a volume
+    plan against FP64 restatements with the same KB operator (W enters A^H W A and A^H W y)."""
+    from test_gpu_operator import _oracle_reliable_cg
+    traj, x, s, n, g, c, j = volume_case("vol64c8")
+    plan = _plan("vol64c8")
+    y = volume_measurement("vol64c8")
+    w = synth.ramp_density(traj)
+    yt, st, wt = torch.from_numpy(y).cuda(), torch.from_numpy(s).cuda(), torch.from_numpy(w).cuda()
+    op = oop.KbSenseOperator3(traj, n, g, j, workers=8)
+    fwd = lambda v: op.forward(v, s)
+    adj = lambda v: op.adjoint(v, s)
+    w64 = w.astype(np.float64)
+    xo, _ = _oracle_reliable_cg(fwd, adj, y, w64, 10, 1e-4, 0, "restart")
+    xg, _, status = plan.cg_sense(yt, st, density=wt, lam=1e-4, iters=10)
+    assert status["finite"] and status["positive_curvature"]
+    assert oop.magnitude_nrmse(xg.cpu().numpy(), xo) <= 2e-3
+    xr_o, res_o = _oracle_reliable_cg(fwd, adj, y, w64, 10, 1e-4, 4, "restart")
+    xr, hist, status = plan.cg_sense(yt, st, density=wt, lam=1e-4, iters=10, reliable_update_period=4,
+                                     reliable_update_direction="restart")
+    assert status["finite"] and status["completed_iterations"] == 10
+    assert oop.magnitude_nrmse(xr.cpu().numpy(), xr_o) <= 2e-3
+    np.testing.assert_allclose(hist[:4], res_o[:4], rtol=2e-3)
+
+
+def test_two_volume_batch_on_slices_matches_single_solves():
+    from trajsparsenufft_b200.operator import Batch
+    a, b = _plan("vol64"), _plan("vol64c8")
+    ta, xa, sa, *_ = volume_case("vol64")
+    tb, xb, sb, *_ = volume_case("vol64c8")
+    ya, yb = torch.from_numpy(volume_measurement("vol64")).cuda(), torch.from_numpy(volume_measurement("vol64c8")).cuda()
+    sa_t, sb_t = torch.from_numpy(sa).cuda(), torch.from_numpy(sb).cuda()
+    single_a, _, _ = a.cg_sense(ya, sa_t, lam=1e-4, iters=5)
+    single_b, _, _ = b.cg_sense(yb, sb_t, lam=1e-4, iters=5)
+    outs, statuses = Batch([a, b], streams=2).cg_sense([ya, yb], [sa_t, sb_t], lam=1e-4, iters=5)
+    assert all(st_["finite"] for st_ in statuses)
+    assert torch.equal(outs[0], single_a) and torch.equal(outs[1], single_b)

@@ -89,10 +89,13 @@ def vd_spiral(interleaves: int, samples: int, exponent: float = 1.5, turns: floa
 
 
 def ramp_density(trajectory: np.ndarray, readout: int | None = None) -> np.ndarray:
-    """[M] float32 ramp density compensation |k| (floored at one readout step), max 1."""
-    k = np.linalg.norm(np.asarray(trajectory, dtype=np.float64).reshape(-1, 2), axis=1)
+    """[M] float32 ramp density compensation, max 1: |k| for [M, 2] trajectories and |k|^2
+    for [M, 3] (3D radial), with |k| floored at half a readout step."""
+    traj = np.asarray(trajectory, dtype=np.float64)
+    dims = traj.shape[-1] if traj.ndim == 2 and traj.shape[-1] in (2, 3) else 2
+    k = np.linalg.norm(traj.reshape(-1, dims), axis=1)
     floor = 1.0 / (readout if readout else 512)
-    w = np.maximum(k, 0.5 * floor)
+    w = np.maximum(k, 0.5 * floor) ** (dims - 1)
     return (w / w.max()).astype(np.float32)
 
 
