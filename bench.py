@@ -642,7 +642,7 @@ def run_grad(args, cfg) -> dict | None:
     g_fwd, _ = capture(fwd_body, False)
     # the graph replays the eager step's kernels: its gradients match an eager step's
     g_grad.replay()
-    loss_e, leaves_e = grad_step()
+    _, leaves_e = grad_step()
     torch.cuda.synchronize()
     eager_leaves = [trip[k] for k in range(3) for trip in leaves_e]  # all y, all maps, all x0: as `leaves`
     graph_vs_eager = max(

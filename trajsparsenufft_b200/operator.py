@@ -172,7 +172,6 @@ class Plan:
         """
         torch = _torch()
         cf = torch.complex64
-        n = self.im_size
         yp = _dev_ptr(y, cf, (self.coils, self.samples), "y")
         sp = _dev_ptr(smaps, cf, self.maps_shape, "smaps")
         dp = None if density is None else _dev_ptr(density, torch.float32, (self.samples,), "density")
@@ -290,7 +289,6 @@ class Batch:
             outs = [torch.empty(pl.image_shape, dtype=cf, device=y.device) for pl, y in zip(self.plans, ys)]
         yp, sp, dp, xp = [], [], [], []
         for i, pl in enumerate(self.plans):
-            n = pl.im_size
             yp.append(_dev_ptr(ys[i], cf, (pl.coils, pl.samples), f"ys[{i}]").value)
             sp.append(_dev_ptr(smaps[i], cf, pl.maps_shape, f"smaps[{i}]").value)
             w = None if densities is None else densities[i]
