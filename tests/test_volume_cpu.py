@@ -81,3 +81,47 @@ def test_volume_phantom_and_maps(n):
     assert x.shape == (n, n, n) and x.dtype == np.complex64 and np.abs(x).max() > 0.1
     assert s.shape == (8, n, n, n)
     assert np.allclose(np.sqrt(np.sum(np.abs(s) ** 2, axis=0)), 1.0, atol=1e-5)
+
+
+@pytest.mark.parametrize("kw,kind", [
+    (dict(grid_size=512, im_size=256), "UNSUPPORTED"),          # 512^3 cells > 2^24 record rows
+    (dict(reference_layout=True), "UNSUPPORTED"),              # volumes use the centred layout
+])
+def test_volume_plan_refusals_before_any_device_work(kw, kind):
+    """Volume plans that the library cannot serve are refused with a status before any CUDA
+    call, so these run without a GPU."""
+    from trajsparsenufft_b200._lib import TsnError
+    from trajsparsenufft_b200.operator import Plan
+    args = dict(im_size=64, grid_size=128, coils=4, width=4, device=0)
+    args.update(kw)
+    with pytest.raises(TsnError) as e:
+        Plan.from_trajectory(synth.kooshball(8, 16), **args)
+    assert e.value.kind == kind
+
+
+def test_volume_trajectory_and_dims_validation():
+    from trajsparsenufft_b200 import _lib
+    from trajsparsenufft_b200._lib import TsnError
+    from trajsparsenufft_b200.operator import Plan, plan_desc
+    bad = synth.kooshball(8, 16) * 1.5                          # outside [-0.5, 0.5]
+    with pytest.raises(TsnError) as e:
+        Plan.from_trajectory(bad, im_size=64, grid_size=128, coils=4, width=4, device=0)
+    assert e.value.kind == "ARG"
+    d = plan_desc(64, 128, 4, 4, dims=4, device=0)
+    t = np.ascontiguousarray(synth.kooshball(8, 16))
+    import ctypes as C
+    h = C.c_void_p()
+    rc = _lib.lib().tsn_plan_create_from_trajectory(t.ctypes.data_as(C.POINTER(C.c_float)), len(t), C.byref(d),
+                                                    C.byref(h))
+    assert _lib.STATUS[rc] == "ARG" and not h.value
+
+
+def test_pack_directories_are_refused_for_volumes():
+    import ctypes as C
+    from trajsparsenufft_b200 import _lib
+    from trajsparsenufft_b200.operator import plan_desc
+    d = plan_desc(64, 128, 4, 4, dims=3, device=0)
+    h = C.c_void_p()
+    rc = _lib.lib().tsn_plan_create_from_pack(b"/nonexistent/r", b"/nonexistent/i", None, None, None, C.byref(d),
+                                              C.byref(h))
+    assert _lib.STATUS[rc] == "UNSUPPORTED" and not h.value
