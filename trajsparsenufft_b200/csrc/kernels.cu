@@ -66,11 +66,12 @@ __device__ __forceinline__ int32_t record_row(const uint8_t* rows24, int32_t fla
 // Records are fetched kRecAhead tiles ahead, gathers kGatherAhead tiles ahead (the gather
 // needs the record's column ids), so a warp waits only on cp.async groups, never on a
 // register load.  Warps are persistent: each streams a contiguous, tile-balanced run of
-// work items and the pipeline runs across item boundaries.  A three-stage ring (34 KB per
-// 4-warp CTA) keeps 24 warps per SM resident, which measured faster than deeper rings
-// with fewer warps (four stages / 20 warps: 1.2% slower solves).
-constexpr int kStages = 3;
-constexpr int kRecAhead = 2;
+// work items and the pipeline runs across item boundaries.  The ring depth STAGES is per
+// view (InterpView::stages): three stages (34 KB per 4-warp CTA, 24 warps per SM) when the
+// gathered panel sits in L2, which measured faster than deeper rings with fewer warps;
+// four stages (45 KB, 20 warps per SM, records one tile further ahead) when it does not and
+// gathers wait on DRAM (3D grids: 1.33 vs 1.79 ms per forward launch).  Records run
+// STAGES - 1 tiles ahead, gathers kGatherAhead.
 constexpr int kGatherAhead = 1;
 
 // Writes one finished item: split chunks publish their accumulators and the last chunk of
@@ -164,9 +165,11 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
   }
 }
 
-template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, int STAGES>
 __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpView v, const __half* __restrict__ panel,
                                                                          InterpOut o) {
+  constexpr int kStages = STAGES;
+  constexpr int kRecAhead = STAGES - 1;
   constexpr int BYTES = ROWH * 2;
   constexpr int CH = BYTES / 16;
   constexpr int NB = ROWH / 8;
@@ -305,13 +308,19 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   cp_async_wait<0>();
 }
 
-template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
-static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, int STAGES>
+static void launch_interp_s(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
   const int blocks = (v.n_warps + kInterpWarps - 1) / kInterpWarps;
-  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (record_bytes(NCOMP) + 32 * ROWH * 2);
-  auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ>;
+  const size_t smem = static_cast<size_t>(kInterpWarps) * STAGES * (record_bytes(NCOMP) + 32 * ROWH * 2);
+  auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ, STAGES>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (blocks > 0) k<<<blocks, kInterpWarps * 32, smem, s>>>(v, panel, o);
+}
+
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
+static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
+  if (v.stages == 4) launch_interp_s<ROWH, SPLIT, NCOMP, EPI, CONJ, 4>(v, panel, o, s);
+  else launch_interp_s<ROWH, SPLIT, NCOMP, EPI, CONJ, 3>(v, panel, o, s);
 }
 
 template <int ROWH>
@@ -330,26 +339,31 @@ static void dispatch_epi(const InterpView& v, const __half* panel, int epi, bool
 
 static int sm_count();
 
-template <int ROWH, int NCOMP>
-static int resident_warps_t() {
-  const size_t smem = static_cast<size_t>(kInterpWarps) * kStages * (record_bytes(NCOMP) + 32 * ROWH * 2);
-  auto k = interp_mmasp_kernel<ROWH, true, NCOMP, EPI_GRID, NCOMP == 2>;
+template <int ROWH, int NCOMP, int STAGES>
+static int resident_warps_s() {
+  const size_t smem = static_cast<size_t>(kInterpWarps) * STAGES * (record_bytes(NCOMP) + 32 * ROWH * 2);
+  auto k = interp_mmasp_kernel<ROWH, true, NCOMP, EPI_GRID, NCOMP == 2, STAGES>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kInterpWarps * 32, smem);
   return std::max(1, per_sm) * kInterpWarps * sm_count();
 }
 
-int interp_resident_warps(int rowh, int ncomp) {
+template <int ROWH, int NCOMP>
+static int resident_warps_t(int stages) {
+  return stages == 4 ? resident_warps_s<ROWH, NCOMP, 4>() : resident_warps_s<ROWH, NCOMP, 3>();
+}
+
+int interp_resident_warps(int rowh, int ncomp, int stages) {
   switch (rowh * 4 + ncomp) {
-    case 16 * 4 + 1: return resident_warps_t<16, 1>();
-    case 16 * 4 + 2: return resident_warps_t<16, 2>();
-    case 32 * 4 + 1: return resident_warps_t<32, 1>();
-    case 32 * 4 + 2: return resident_warps_t<32, 2>();
-    case 48 * 4 + 1: return resident_warps_t<48, 1>();
-    case 48 * 4 + 2: return resident_warps_t<48, 2>();
-    case 64 * 4 + 1: return resident_warps_t<64, 1>();
-    default: return resident_warps_t<64, 2>();
+    case 16 * 4 + 1: return resident_warps_t<16, 1>(stages);
+    case 16 * 4 + 2: return resident_warps_t<16, 2>(stages);
+    case 32 * 4 + 1: return resident_warps_t<32, 1>(stages);
+    case 32 * 4 + 2: return resident_warps_t<32, 2>(stages);
+    case 48 * 4 + 1: return resident_warps_t<48, 1>(stages);
+    case 48 * 4 + 2: return resident_warps_t<48, 2>(stages);
+    case 64 * 4 + 1: return resident_warps_t<64, 1>(stages);
+    default: return resident_warps_t<64, 2>(stages);
   }
 }
 

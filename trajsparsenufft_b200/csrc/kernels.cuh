@@ -68,6 +68,7 @@ struct InterpView {
   int32_t groups = 0;
   int32_t ncomp = 0;
   int32_t rec_bytes = 0;
+  int32_t stages = 3;                   // per-warp ring depth: 3, or 4 when the gathered panel exceeds L2
 };
 constexpr int kPartialFloats = 32;  // >= NCOMP * NA * 4 for every instantiation
 
@@ -120,7 +121,7 @@ void launch_interp(const InterpView& v, const __half* panel, int rowh, bool spli
                    const InterpOut& o, cudaStream_t s);
 // warps the persistent interpolation kernel keeps resident on this device for a panel row
 // width / component count (used to cut the item list into per-warp runs)
-int interp_resident_warps(int rowh, int ncomp);
+int interp_resident_warps(int rowh, int ncomp, int stages);
 constexpr int kInterpWarpsPerCta = 4;
 
 void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t s);

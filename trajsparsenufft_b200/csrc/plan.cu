@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstring>
 #include <initializer_list>
+#include <iterator>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -213,6 +214,8 @@ std::vector<int2> cut_ranges(const std::vector<int64_t>& item_ends, int64_t tile
   return ranges;
 }
 
+constexpr int64_t kLocalityPanelBytes = 64ll << 20;  // about half of the 126 MB L2
+
 void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
   DevView& d = P->view[which];
   const int64_t tiles = h.tiles(), groups = h.groups();
@@ -244,14 +247,25 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
     slots += nch;
     ++nsplit;
   }
-  // stream order: each chunk of a split group (the long poles, first in their run) is followed
-  // by whole small groups up to the average run length, so runs can be cut close to the
-  // average instead of at multiples of the chunk length
-  {
+  // stream order. When the gathered panel is much larger than L2 (volume grids, large sample
+  // sets), items stay in row-group (Morton) order with each split group's chunks in place:
+  // consecutive groups share panel rows, and a warp's contiguous run then finds them in L2.
+  // Otherwise each chunk of a split group (the long poles, first in their run) is followed by
+  // whole small groups up to the average run length, so runs can be cut close to the average
+  // instead of at multiples of the chunk length.
+  const bool large_panel = h.n_cols * 8 * static_cast<int64_t>(P->C) > kLocalityPanelBytes;
+  const int stages = large_panel ? 4 : 3;
+  if (large_panel) {
+    std::vector<Item> all;
+    all.reserve(items.size() + small.size());
+    std::merge(items.begin(), items.end(), small.begin(), small.end(), std::back_inserter(all),
+               [](const Item& a, const Item& b) { return a.group < b.group || (a.group == b.group && a.chunk < b.chunk); });
+    items.swap(all);
+  } else {
     int64_t total = 0;
     for (const Item& it : items) total += it.t1 - it.t0;
     for (const Item& it : small) total += it.t1 - it.t0;
-    const int warps_full = interp_resident_warps(4 * P->C, ncomp);
+    const int warps_full = interp_resident_warps(4 * P->C, ncomp, stages);
     const double avg = static_cast<double>(total) / std::max(1, warps_full);
     std::vector<Item> order;
     order.reserve(items.size() + small.size());
@@ -311,7 +325,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
     d.item_ends.push_back(pos);
   }
   if (pos != tiles) fail(TSN_ERR_FORMAT, "group offsets do not cover the tiles");
-  const std::vector<int2> ranges = cut_ranges(d.item_ends, tiles, interp_resident_warps(4 * P->C, ncomp));
+  const std::vector<int2> ranges = cut_ranges(d.item_ends, tiles, interp_resident_warps(4 * P->C, ncomp, stages));
   d.records.upload(records);
   d.counters.upload(std::vector<int32_t>(std::max(nsplit, 1), 0));
   d.partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kPartialFloats * 32);
@@ -324,6 +338,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   d.v.groups = static_cast<int32_t>(groups);
   d.v.ncomp = ncomp;
   d.v.rec_bytes = rec;
+  d.v.stages = stages;
   d.tiles = tiles;
   d.groups = groups;
   d.active_rows = h.active_rows;
@@ -807,7 +822,7 @@ void prepare_share(tsn_plan* P, int share) {
   if (share <= 1) return;
   for (DevView& d : P->view) {
     if (!d.present || d.share == share) continue;
-    const int warps = std::max(kInterpWarpsPerCta, interp_resident_warps(4 * P->C, d.v.ncomp) / share);
+    const int warps = std::max(kInterpWarpsPerCta, interp_resident_warps(4 * P->C, d.v.ncomp, d.v.stages) / share);
     const std::vector<int2> ranges = cut_ranges(d.item_ends, d.tiles, warps);
     d.ranges_shared.upload(ranges);
     d.v_shared = d.v;
