@@ -248,19 +248,15 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
     ++nsplit;
   }
   // stream order. When the gathered panel is much larger than L2 (volume grids, large sample
-  // sets), items stay in row-group (Morton) order with each split group's chunks in place:
-  // consecutive groups share panel rows, and a warp's contiguous run then finds them in L2.
-  // Otherwise each chunk of a split group (the long poles, first in their run) is followed by
-  // whole small groups up to the average run length, so runs can be cut close to the average
-  // instead of at multiples of the chunk length.
+  // sets), the chunks of split groups come first and the whole small groups after them, each
+  // list in row-group (Morton) order: consecutive groups share panel rows, and a warp's
+  // contiguous run then finds them in L2. Otherwise each chunk of a split group (the long
+  // poles, first in their run) is followed by whole small groups up to the average run length,
+  // so runs can be cut close to the average instead of at multiples of the chunk length.
   const bool large_panel = h.n_cols * 8 * static_cast<int64_t>(P->C) > kLocalityPanelBytes;
   const int stages = large_panel ? 4 : 3;
   if (large_panel) {
-    std::vector<Item> all;
-    all.reserve(items.size() + small.size());
-    std::merge(items.begin(), items.end(), small.begin(), small.end(), std::back_inserter(all),
-               [](const Item& a, const Item& b) { return a.group < b.group || (a.group == b.group && a.chunk < b.chunk); });
-    items.swap(all);
+    items.insert(items.end(), small.begin(), small.end());
   } else {
     int64_t total = 0;
     for (const Item& it : items) total += it.t1 - it.t0;
