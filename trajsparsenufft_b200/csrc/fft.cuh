@@ -8,7 +8,8 @@
 //   3. transpose through a padded per-warp shared buffer,
 //   4. 32-point DFTs over l, each split across T = 32/P lanes: a P-point register DFT
 //      per lane, twiddle W_32^(h m), then a T-point DFT across the T lanes by shuffles.
-// Output: lane (k = lane / T, h = lane % T) holds X[k + P m + P^2 h] in register m.
+// Output: lane (k = lane / T, h = lane % T) holds X[k + P q + P^2 k3] in register m, with
+// (q, k3) from the cross-lane step (warp_fft_pow2_out_index).
 // Forward = exp(-2 pi i nk/G), inverse = exp(+2 pi i nk/G), both unnormalized.
 // Twiddles are FP64-computed, FP32-stored tables (host fills them once per plan).
 // The reference's FFT endpoints are SIMT FP32 shared-memory radix-8/16/32 kernels
@@ -138,52 +139,71 @@ __device__ __forceinline__ void warp_fft_pow2(float2 (&v)[G / 32], float2* scrat
         v[m] = h == 0 ? cadd(v[m], o) : csub(o, v[m]);
       }
     } else if (T == 4) {
-      // X_h = sum_{h2} Z_{h2} W_4^{h2 h}, W_4 = -i (forward) / +i (inverse)
+      // The 4-point DFTs across lanes go through the warp scratch instead of shuffles: lane
+      // (kk, h) takes the Q = P/4 columns m = h Q + i and, for each, the values of the four
+      // lanes kk*4 + h2. Rows are XOR-swizzled by the column group m / Q, which makes both the
+      // row writes and these reads conflict-free. Then a register DFT-4 per column.
+      constexpr int Q = P / 4;
+      __syncwarp();
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        float2 z[4];
+      for (int m = 0; m < P; ++m) scratch[m * 32 + (lane ^ (m / Q))] = v[m];
+      __syncwarp();
+      float2 u[Q][4];
 #pragma unroll
-        for (int h2 = 0; h2 < 4; ++h2) {
-          z[h2].x = __shfl_sync(0xFFFFFFFFu, v[m].x, (lane & ~3) | h2);
-          z[h2].y = __shfl_sync(0xFFFFFFFFu, v[m].y, (lane & ~3) | h2);
-        }
-        const float2 s02 = cadd(z[0], z[2]), d02 = csub(z[0], z[2]);
-        const float2 s13 = cadd(z[1], z[3]), d13 = csub(z[1], z[3]);
-        // forward: X1 = d02 - i d13, X3 = d02 + i d13 ; inverse swaps
-        const float2 mi_d13 = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
-        float2 r;
-        if (h == 0) r = cadd(s02, s13);
-        else if (h == 1) r = cadd(d02, mi_d13);
-        else if (h == 2) r = csub(s02, s13);
-        else r = csub(d02, mi_d13);
-        v[m] = r;
+      for (int i = 0; i < Q; ++i)
+#pragma unroll
+        for (int h2 = 0; h2 < 4; ++h2) u[i][h2] = scratch[(h * Q + i) * 32 + ((kk * 4 + h2) ^ h)];
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        dft_reg<4, INV>(u[i]);
+#pragma unroll
+        for (int k3 = 0; k3 < 4; ++k3) v[i * 4 + k3] = u[i][k3];
       }
     } else {
-      // T == 8 (P == 4): radix-8 across lanes by direct summation
+      // T == 8 (P == 4): each 8-point DFT across lanes is split over a lane pair. Lane (kk, h)
+      // takes column m = h / 2 and the four values of lanes kk*8 + 2 j + e (e = h % 2) from the
+      // scratch (XOR swizzle 2m: conflict-free), a register DFT-4 gives the even (e = 0) or odd
+      // (e = 1) half, the odd half is multiplied by W_8^k, and one shuffle exchange across the
+      // pair forms X[k] = E[k] + W_8^k O[k] (e = 0) and X[k + 4] = E[k] - W_8^k O[k] (e = 1).
+      __syncwarp();
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        float2 acc = make_float2(0.f, 0.f);
+      for (int m = 0; m < P; ++m) scratch[m * 32 + (lane ^ (2 * m))] = v[m];
+      __syncwarp();
+      const int mm = h >> 1, e = h & 1;
+      float2 u[4];
 #pragma unroll
-        for (int h2 = 0; h2 < 8; ++h2) {
-          float2 z;
-          z.x = __shfl_sync(0xFFFFFFFFu, v[m].x, (lane & ~7) | h2);
-          z.y = __shfl_sync(0xFFFFFFFFu, v[m].y, (lane & ~7) | h2);
-          float2 w = tw[TS * (((h2 * h) & 7) * (G / 8))];
-          if (INV) w.y = -w.y;
-          acc = cadd(acc, cmul(z, w));
-        }
-        v[m] = acc;
+      for (int j = 0; j < 4; ++j) u[j] = scratch[mm * 32 + ((kk * 8 + 2 * j + e) ^ (2 * mm))];
+      __syncwarp();
+      dft_reg<4, INV>(u);
+#pragma unroll
+      for (int k = 1; k < 4; ++k)
+        if (e) u[k] = cmul(u[k], const_twiddle<INV>(k * 128));  // W_8^k = exp(-2 pi i k / 8)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float2 o;
+        o.x = __shfl_xor_sync(0xFFFFFFFFu, u[k].x, 1);
+        o.y = __shfl_xor_sync(0xFFFFFFFFu, u[k].y, 1);
+        v[k] = e ? csub(o, u[k]) : cadd(u[k], o);
       }
     }
   }
 }
 
-// Output element index held in register m after warp_fft_pow2<G>.
+// Output element index held in register m after warp_fft_pow2<G>: lane (kk = lane / T,
+// h = lane % T) holds X[kk + P q + P^2 k3] with, by the cross-lane step,
+//   T <= 2: q = m, k3 = h;
+//   T == 4: q = h (P/4) + m / 4, k3 = m % 4;
+//   T == 8: q = h / 2, k3 = m + 4 (h % 2).
 template <int G>
 __device__ __forceinline__ int warp_fft_pow2_out_index(int m) {
   using S = WarpFftShape<G>;
+  constexpr int P = S::P, T = S::T;
   const int lane = threadIdx.x & 31;
-  return lane / S::T + S::P * m + S::P * S::P * (lane % S::T);
+  const int kk = lane / T, h = lane % T;
+  if constexpr (T == 4) return kk + P * (h * (P / 4) + m / 4) + P * P * (m % 4);
+  else if constexpr (T == 8) return kk + P * (h >> 1) + P * P * (m + 4 * (h & 1));
+  else return kk + P * m + P * P * h;
 }
 
 // Lengths G = R * B with R in {1, 3, 5} and a power-of-two base B = 32 * 2^k >= 128; the
