@@ -96,7 +96,9 @@ struct GraphKey {
   }
 };
 
-std::once_flag g_const_once;
+// __constant__ twiddle tables are per device: filled once for each device a plan lives on
+std::mutex g_const_mutex;
+std::vector<int> g_const_devices;
 
 }  // namespace
 
@@ -413,7 +415,15 @@ void allocate_workspaces(tsn_plan* P) {
   P->info.dims = P->dims;
   P->info.workspace_bytes = static_cast<int64_t>(P->z1.bytes + P->z2.bytes + P->panel.bytes + P->spanel.bytes +
                                                  P->grid.bytes + 4 * P->r.bytes + P->state.bytes);
-  std::call_once(g_const_once, []() { set_twiddle_constants(nullptr); });
+  {
+    std::lock_guard<std::mutex> lock(g_const_mutex);
+    int dev = 0;
+    CUDA_OK(cudaGetDevice(&dev));
+    if (std::find(g_const_devices.begin(), g_const_devices.end(), dev) == g_const_devices.end()) {
+      set_twiddle_constants(nullptr);
+      g_const_devices.push_back(dev);
+    }
+  }
   CUDA_OK(cudaGetLastError());
 }
 
