@@ -25,6 +25,17 @@ namespace dev {
 // (included by exactly one translation unit)
 __constant__ float2 c_w1024[1024];
 
+// exp(-2 pi i j / R) for R = 3 and 5, filled with the plan twiddle tables' FP64 expression
+// (so equal to tw[B j] of a G = R B plan): uniform across lanes, read as constant operands
+__constant__ float2 c_wr3[3];
+__constant__ float2 c_wr5[5];
+
+template <int R, bool INV>
+__device__ __forceinline__ float2 radix_twiddle(int j) {
+  const float2 w = R == 3 ? c_wr3[j] : c_wr5[j];
+  return INV ? make_float2(w.x, -w.y) : w;
+}
+
 template <bool INV>
 __device__ __forceinline__ float2 const_twiddle(int e1024) {
   const float2 w = c_w1024[e1024 & 1023];
@@ -270,8 +281,7 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, c
         float2 acc = t[0];
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          float2 w = tw[B * ((r * q) % R)];  // W_R^{r q} = W_G^{B (r q mod R)}
-          if (INV) w.y = -w.y;
+          const float2 w = radix_twiddle<R, INV>((r * q) % R);  // W_R^{r q}, a constant operand
           acc = cadd(acc, cmul(t[r], w));
         }
         v[q * PB + m] = acc;

@@ -30,6 +30,19 @@ void set_twiddle_constants(cudaStream_t s) {
     w[e] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
   }
   cudaMemcpyToSymbolAsync(dev::c_w1024, w.data(), sizeof(float2) * 1024, 0, cudaMemcpyHostToDevice, s);
+  // W_R^j with the plan tables' expression (-2 pi e) / G at e = B j, G = R B: for a power-of-two
+  // B that is exactly (-2 pi j) / R, so these equal the plans' tw[B j]
+  float2 w3[3], w5[5];
+  for (int j = 0; j < 3; ++j) {
+    const double a = -2.0 * M_PI * j / 3.0;
+    w3[j] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+  }
+  for (int j = 0; j < 5; ++j) {
+    const double a = -2.0 * M_PI * j / 5.0;
+    w5[j] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+  }
+  cudaMemcpyToSymbolAsync(dev::c_wr3, w3, sizeof w3, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(dev::c_wr5, w5, sizeof w5, 0, cudaMemcpyHostToDevice, s);
   cudaStreamSynchronize(s);
 }
 
