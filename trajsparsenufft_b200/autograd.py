@@ -44,8 +44,11 @@ class PlanOps:
 
 
 def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
-    """Re <a, b> in FP64 (a 0-d tensor)."""
-    return torch.vdot(a.reshape(-1), b.reshape(-1)).real.to(torch.float64)
+    """Re <a, b> = sum(a.re b.re + a.im b.im), accumulated in FP64 (a 0-d tensor), like the graph
+    solver's CG inner products (a complex64 vdot would accumulate in FP32)."""
+    ar = torch.view_as_real(a.reshape(-1)).reshape(-1).to(torch.float64)
+    br = torch.view_as_real(b.reshape(-1)).reshape(-1).to(torch.float64)
+    return torch.dot(ar, br)
 
 
 class _Sense:
