@@ -120,11 +120,23 @@ __device__ __forceinline__ void warp_fft_pow2(float2 (&v)[G / 32], float2* scrat
   constexpr int P = S::P, T = S::T;
   const int lane = threadIdx.x & 31;
   dft_reg<P, INV>(v);
+  // twiddles W_G^(lane k): the power-of-two exponents come from the table, the others are
+  // products of at most three of them (W^k = W^(high bit of k) W^(rest)), which trades shared
+  // memory loads for FP32 multiplies at an error of a few ulp
+  {
+    float2 wk[P];
+    wk[0] = make_float2(1.f, 0.f);
 #pragma unroll
-  for (int k = 1; k < P; ++k) {
-    float2 w = tw[TS * ((lane * k) & (G - 1))];
-    if (INV) w.y = -w.y;
-    v[k] = cmul(v[k], w);
+    for (int k = 1; k < P; ++k) {
+      if ((k & (k - 1)) == 0) {
+        wk[k] = tw[TS * ((lane * k) & (G - 1))];
+        if (INV) wk[k].y = -wk[k].y;
+      } else {
+        const int hb = 1 << (31 - __clz(k));
+        wk[k] = cmul(wk[hb], wk[k - hb]);
+      }
+      v[k] = cmul(v[k], wk[k]);
+    }
   }
 #pragma unroll
   for (int k = 0; k < P; ++k) scratch[k * S::PITCH + lane] = v[k];
