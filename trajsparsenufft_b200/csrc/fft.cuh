@@ -147,11 +147,19 @@ __device__ __forceinline__ void warp_fft_pow2(float2 (&v)[G / 32], float2* scrat
   __syncwarp();
   dft_reg<P, INV>(v);
   if (T > 1) {
+    // W_G^(h m P): loaded at power-of-two m, products of at most two of those otherwise
+    float2 wm[P];
+    wm[0] = make_float2(1.f, 0.f);
 #pragma unroll
     for (int m = 1; m < P; ++m) {
-      float2 w = tw[TS * ((h * m * P) & (G - 1))];
-      if (INV) w.y = -w.y;
-      v[m] = cmul(v[m], w);
+      if ((m & (m - 1)) == 0) {
+        wm[m] = tw[TS * ((h * m * P) & (G - 1))];
+        if (INV) wm[m].y = -wm[m].y;
+      } else {
+        const int hb = 1 << (31 - __clz(m));
+        wm[m] = cmul(wm[hb], wm[m - hb]);
+      }
+      v[m] = cmul(v[m], wm[m]);
     }
     if (T == 2) {
 #pragma unroll
@@ -282,12 +290,20 @@ __device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], float2* scratch, c
       const int k = warp_fft_pow2_out_index<B>(m);
       float2 t[R];
       t[0] = v[m];
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = tw[r * k];  // r k < G
-        if (INV) w.y = -w.y;
-        t[r] = cmul(v[r * PB + m], w);
+      // W_G^(r k), r < R: W^k and (R == 5) W^2k from the table, the rest as products
+      float2 wr[R];
+      wr[1] = tw[k];
+      if (INV) wr[1].y = -wr[1].y;
+      if constexpr (R == 3) {
+        wr[2] = cmul(wr[1], wr[1]);
+      } else {
+        wr[2] = tw[2 * k];  // 2 k < G
+        if (INV) wr[2].y = -wr[2].y;
+        wr[3] = cmul(wr[2], wr[1]);
+        wr[4] = cmul(wr[2], wr[2]);
       }
+#pragma unroll
+      for (int r = 1; r < R; ++r) t[r] = cmul(v[r * PB + m], wr[r]);
 #pragma unroll
       for (int q = 0; q < R; ++q) {
         float2 acc = t[0];
