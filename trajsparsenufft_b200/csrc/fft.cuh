@@ -147,19 +147,11 @@ __device__ __forceinline__ void warp_fft_pow2(float2 (&v)[G / 32], float2* scrat
   __syncwarp();
   dft_reg<P, INV>(v);
   if (T > 1) {
-    // W_G^(h m P): loaded at power-of-two m, products of at most two of those otherwise
-    float2 wm[P];
-    wm[0] = make_float2(1.f, 0.f);
 #pragma unroll
     for (int m = 1; m < P; ++m) {
-      if ((m & (m - 1)) == 0) {
-        wm[m] = tw[TS * ((h * m * P) & (G - 1))];
-        if (INV) wm[m].y = -wm[m].y;
-      } else {
-        const int hb = 1 << (31 - __clz(m));
-        wm[m] = cmul(wm[hb], wm[m - hb]);
-      }
-      v[m] = cmul(v[m], wm[m]);
+      float2 w = tw[TS * ((h * m * P) & (G - 1))];
+      if (INV) w.y = -w.y;
+      v[m] = cmul(v[m], w);
     }
     if (T == 2) {
 #pragma unroll
