@@ -555,6 +555,16 @@ HostView host_view_batched(const SparseView& v, const tsn_plan_desc* d) {
       }
     }
     const CompressedTiles ct = compress_tiles(tiles);
+    if (g0 == 0 && g1 < n_groups) {
+      // reserve once from the first batch's tiles per group (+25%): growing by doubling would
+      // touch fresh memory again at every step, which dominates planning time on hosts where
+      // first touch is slow
+      const double per_group = static_cast<double>(tiles.size()) / static_cast<double>(g1 - g0);
+      const size_t est = static_cast<size_t>(per_group * static_cast<double>(n_groups) * 1.25) + 1;
+      h.tile_col_ids.reserve(est * kKTile);
+      h.a[0].reserve(est * kMTile * (kKTile / 2));
+      h.meta[0].reserve(est * kMTile);
+    }
     h.tile_col_ids.insert(h.tile_col_ids.end(), ct.col_ids.begin(), ct.col_ids.end());
     h.a[0].insert(h.a[0].end(), ct.values.begin(), ct.values.end());
     h.meta[0].insert(h.meta[0].end(), ct.pair_meta.begin(), ct.pair_meta.end());
