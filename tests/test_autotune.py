@@ -51,6 +51,14 @@ def test_trajectory_key_is_stable_and_shape_sensitive():
     assert k != autotune.trajectory_key(t[:-1], 64, 128, 4, 6, "dev")
 
 
+def test_volume_trajectory_key():
+    v = synth.kooshball(7, 9)                      # 63 samples: 189 values, not a multiple of 2
+    k = autotune.trajectory_key(v, 64, 128, 4, 4, "dev")
+    assert k == autotune.trajectory_key(v.astype(np.float64), 64, 128, 4, 4, "dev")
+    flat = v.reshape(-1)[:126].reshape(-1, 2)       # the same leading bytes as an image trajectory
+    assert k != autotune.trajectory_key(flat, 64, 128, 4, 4, "dev")
+
+
 @pytest.mark.gpu
 def test_autotuned_plan_on_gpu(tmp_path):
     pytest.importorskip("torch")

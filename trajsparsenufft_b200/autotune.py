@@ -34,10 +34,16 @@ def cache_path() -> Path:
 
 
 def trajectory_key(trajectory, im_size: int, grid_size: int, coils: int, width: int, device_name: str = "") -> str:
-    t = np.ascontiguousarray(np.asarray(trajectory, dtype=np.float32).reshape(-1, 2))
+    """SHA-256 of the float32 trajectory and the plan shape; [M, 3] (volume) trajectories add a
+    dimension tag, so an image and a volume trajectory with the same bytes never share a key."""
+    a = np.asarray(trajectory, dtype=np.float32)
+    dims = 3 if a.ndim == 2 and a.shape[1] == 3 else 2
+    t = np.ascontiguousarray(a.reshape(-1, dims))
     h = hashlib.sha256()
     h.update(t.tobytes())
     h.update(f"|{im_size}|{grid_size}|{coils}|{width}|{device_name}".encode())
+    if dims == 3:
+        h.update(b"|3d")
     return h.hexdigest()
 
 
@@ -60,10 +66,10 @@ def _store(path: Path, key: str, entry: dict) -> None:
 def interp_ms(plan, reps: int = 10) -> float:
     """Forward + adjoint interpolation time per CG iteration of a plan (ms, CUDA events)."""
     import torch
-    n, c = plan.im_size, plan.coils
+    c = plan.coils
     dev = torch.device("cuda", torch.cuda.current_device())
     y = torch.randn(c, plan.samples, dtype=torch.complex64, device=dev)
-    smaps = torch.ones(c, n, n, dtype=torch.complex64, device=dev) / np.sqrt(c)
+    smaps = torch.ones(plan.maps_shape, dtype=torch.complex64, device=dev) / np.sqrt(c)
     st = plan.profile_stages(y, smaps, reps=reps)
     return st["interp_fwd"] + st["interp_adj"]
 
