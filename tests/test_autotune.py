@@ -75,3 +75,20 @@ def test_autotuned_plan_on_gpu(tmp_path):
                                    cache=tmp_path / "t.json")
     assert choice2["cached"] and choice2["policy"] == choice["policy"]
     assert plan2.info["tiles"] == plan.info["tiles"]
+
+
+@pytest.mark.gpu
+def test_autotuned_volume_plan_on_gpu(tmp_path):
+    pytest.importorskip("torch")
+    import sys
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent))
+    from gpu_cases import volume_case
+    traj, x, s, n, g, c, j = volume_case("vol64")
+    cands = [("optimized", "morton"), ("optimized", "trajectory")]
+    plan, choice = autotune.plan(traj, im_size=n, grid_size=g, coils=c, width=j, candidates=cands,
+                                 cache=tmp_path / "v.json")
+    assert plan.dims == 3 and (choice["planner"], choice["policy"]) in cands and not choice["cached"]
+    assert choice["interp_ms"] == min(t["interp_ms"] for t in choice["trials"]) > 0
+    _, choice2 = autotune.plan(traj, im_size=n, grid_size=g, coils=c, width=j, candidates=cands,
+                               cache=tmp_path / "v.json")
+    assert choice2["cached"] and choice2["policy"] == choice["policy"]
