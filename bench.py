@@ -176,15 +176,25 @@ def algorithmic_bytes(plan, cfg: dict) -> dict:
     n, g, c, m = cfg["n"], cfg["g"], cfg["c"], plan.samples
     panel_row = 8 * c            # FP16 hi + res, complex, C coils
     img = n * n * 8
+    # inner CG iterations: the forward rows finish the previous update (r, p, ap, x in; x, r, p
+    # out) and the inverse rows read r for the update's partials
     return {
-        "fwd_rows": img * 2 + c * img + n * n * 4 + g * n * c * 8,          # r, p rw, smaps, scaling, z1 write
+        "fwd_rows": img * 7 + c * img + n * n * 4 + g * n * c * 8,          # r, p, ap, x rw, smaps, scaling, z1
         "fwd_cols": g * n * c * 8 + g * g * panel_row,                       # z1 read, panel write
         "interp_fwd": info["pack_bytes"][0] + g * g * panel_row + m * panel_row,   # pack, panel read, sample panel
         "interp_adj": info["pack_bytes"][1] + m * panel_row + info["active_rows"][1] * c * 8,  # pack, panel, grid
         "inv_cols": g * g * c * 8 + g * n * c * 8,
-        "inv_rows": g * n * c * 8 + c * img + n * n * 4 + img * 2,          # w1, smaps, scaling, p, ap
-        "cg_update": img * 6,
+        "inv_rows": g * n * c * 8 + c * img + n * n * 4 + img * 3,          # w1, smaps, scaling, p, r, ap
+        "cg_update": img * 6,                                                # the last iteration only
     }
+
+
+def solve_bytes(alg: dict, iters: int, img: int, rhs: tuple) -> int:
+    """Compulsory bytes of one solve: `iters` iterations whose forward rows (but the first)
+    finish the previous update, one cg_update after the last, and the right-hand-side stages."""
+    per_iter = sum(v for k, v in alg.items() if k != "cg_update")
+    # the first forward rows reads r and writes p only; the last inverse rows reads no r
+    return iters * per_iter - 5 * img - img + alg["cg_update"] + sum(alg[k] for k in rhs)
 
 
 def run_ours(args, cfg) -> dict:
@@ -328,8 +338,8 @@ def run_ours(args, cfg) -> dict:
     dominant = max(stages, key=stages.get)
     peak, peak_kind = measured_peaks()
     achieved = alg[dominant] / (stages[dominant] * 1e-3) / 1e9
-    per_iter_ms = sum(stages.values())
-    recon_bytes = iters * sum(alg.values()) + alg["interp_adj"] + alg["inv_cols"] + alg["inv_rows"]
+    per_iter_ms = sum(v for k, v in stages.items() if k != "cg_update")
+    recon_bytes = solve_bytes(alg, iters, cfg["n"] ** 2 * 8, ("interp_adj", "inv_cols", "inv_rows"))
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "recons/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
@@ -345,7 +355,7 @@ def run_ours(args, cfg) -> dict:
                 "h2d_ms_per_step": round(h2d_ms, 4),
                 "repeats": [round(job_rate(world, 1, e2e_steps, m), 3) for m in e2e_repeats],
                 "statistic": f"median of {len(e2e_repeats)} runs of {e2e_steps} steps"},
-        "gpu_launches": args.steps * (5 + 7 * iters + 1),
+        "gpu_launches": args.steps * (5 + 6 * iters + 2),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": committed_traffic(dominant),
@@ -528,7 +538,7 @@ def run_batch(args, cfg) -> dict | None:
                 "overlap": "copies of step k+1 overlap the solve of step k",
                 "repeats": [round(job_rate(world, n_cases, e2e_steps, m), 3) for m in e2e_repeats],
                 "statistic": f"median of {len(e2e_repeats)} runs of {e2e_steps} steps"},
-        "gpu_launches": args.steps * n_cases * (5 + 7 * iters + 1),
+        "gpu_launches": args.steps * n_cases * (5 + 6 * iters + 2),
         "clocks": clocks.summary(),
     }
     return out if rank == 0 else None
@@ -793,14 +803,14 @@ def volume_bytes(plan, cfg: dict) -> dict:
     panel_row = 8 * c
     m = plan.samples
     return {
-        "fwd_rows": pix * 8 * 3 + c * pix * 8 + pix * 4 + z1,      # r, p in, p out, smaps, scaling, z1
+        "fwd_rows": pix * 8 * 7 + c * pix * 8 + pix * 4 + z1,      # r, p, ap, x rw, smaps, scaling, z1
         "fwd_mid": z1 + z2,
         "fwd_cols": z2 + g ** 3 * panel_row,
         "interp_fwd": info["pack_bytes"][0] + g ** 3 * panel_row + m * panel_row,
         "interp_adj": info["pack_bytes"][1] + m * panel_row + info["active_rows"][1] * c * 8,
         "inv_cols": g ** 3 * c * 8 + z2,
         "inv_mid": z2 + z1,
-        "inv_rows": z1 + c * pix * 8 + pix * 4 + pix * 8 * 2,       # z1, smaps, scaling, p, ap
+        "inv_rows": z1 + c * pix * 8 + pix * 4 + pix * 8 * 3,       # z1, smaps, scaling, p, r, ap
         "cg_update": pix * 8 * 6,
     }
 
@@ -916,7 +926,7 @@ def run_volume(args, cfg) -> dict | None:
     dominant = max(stages, key=stages.get)
     peak, peak_kind = measured_peaks()
     achieved = alg[dominant] / (stages[dominant] * 1e-3) / 1e9
-    recon_bytes = iters * sum(alg.values())
+    recon_bytes = solve_bytes(alg, iters, n ** 3 * 8, ("interp_adj", "inv_cols", "inv_mid", "inv_rows"))
     m = plan.samples
     out = {
         "metric": VOLUME_METRIC if cfg["n"] == 128 else VOLUME_METRIC.replace("128^3", f"{n}^3"), "value": round(value, 4), "unit": "recons/s", "n_gpus": world, "steps": args.steps,
@@ -936,7 +946,7 @@ def run_volume(args, cfg) -> dict | None:
                 "d2h_bytes_per_step": int(x_out.numel() * 8),
                 "repeats": [round(job_rate(world, 1, e2e_steps, v), 4) for v in e2e_repeats],
                 "statistic": f"median of {len(e2e_repeats)} runs of {e2e_steps} steps"},
-        "gpu_launches": args.steps * (7 + 11 * iters + 1),
+        "gpu_launches": args.steps * (7 + 9 * iters + 3),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
                      "algorithmic_bytes_per_launch": alg[dominant], "launch_ms": round(stages[dominant], 5)},

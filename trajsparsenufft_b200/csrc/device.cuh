@@ -119,6 +119,30 @@ __device__ __forceinline__ double block_sum(double v, double* scratch) {
   return t;
 }
 
+// Three deterministic block sums at once (one pass of barriers); `scratch` holds 99 doubles.
+__device__ __forceinline__ double3 block_sum3(double a, double b, double c, double* scratch) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  c = warp_sum(c);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    scratch[warp] = a;
+    scratch[33 + warp] = b;
+    scratch[66 + warp] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += scratch[33 * threadIdx.x + w];
+    scratch[33 * threadIdx.x + 32] = t;
+  }
+  __syncthreads();
+  const double3 t = make_double3(scratch[32], scratch[65], scratch[98]);
+  __syncthreads();
+  return t;
+}
+
 // Power-of-two scale bringing rms to ~target (FP16 rounding commutes with it).
 __device__ __forceinline__ float pow2_scale(double sum_sq, double count, float target) {
   const double rms = sqrt(sum_sq / count);

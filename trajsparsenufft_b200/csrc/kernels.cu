@@ -421,6 +421,17 @@ __device__ __forceinline__ double sum_partials(const double* part, int nparts, d
   return block_sum(a, scratch);
 }
 
+// Sums of three partial sections [nparts] spaced `stride` apart, as sum_partials does each.
+__device__ __forceinline__ double3 sum_partials3(const double* part, int nparts, int64_t stride, double* scratch) {
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    a += part[i];
+    b += part[stride + i];
+    c += part[2 * stride + i];
+  }
+  return block_sum3(a, b, c, scratch);
+}
+
 // ------------------------------------------------------------------------------------------
 // FFT endpoints. One warp per coil (blockDim = 32*C), one CTA per image row / grid column.
 // ------------------------------------------------------------------------------------------
@@ -468,35 +479,49 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
 //     mode 0 with smaps:  row0 = x row, maps = S_c rows      (row1 unused)
 //     mode 0 without:     maps = coil-image rows
 //     mode 1 (CG):        row0 = r row, row1 = p row, maps = S_c rows
+//     mode 4 (CG, fused update): row0 = r, row1 = p, row2 = A p, row3 = x rows, maps = S_c rows
 //   the per-warp FFT scratch [C][SCR], and the output rows [G][C+1] float2.
-// Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844).
+// Mode 4 also finishes CG iteration iter-1, which then needs no cg_update launch: parts holds
+// three sections [lines] of <p, Ap>, Re <r, Ap> and <Ap, Ap> from the inverse rows, so
+// alpha = rho / pAp, and rho' = |r - alpha Ap|^2 = rho - 2 alpha Re <r, Ap> + alpha^2 <Ap, Ap>
+// (FP64); each row updates x += alpha p and r -= alpha Ap before p = r + beta p.
+// Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844);
+// the CG update of reference_sparse_solver.py:297-323.
 template <int G, int CC>
 __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f, const float2* __restrict__ x, float2* __restrict__ z1,
-                                                     int mode, float2* __restrict__ p, const float2* __restrict__ r,
+                                                     int mode, float2* __restrict__ p, float2* __restrict__ r,
                                                      const double* __restrict__ parts, int nparts,
-                                                     CgState* __restrict__ st, int iter) {
+                                                     CgState* __restrict__ st, int iter, float2* __restrict__ xs,
+                                                     const float2* __restrict__ ap) {
   constexpr int P = G / 32;
   extern __shared__ __align__(16) uint8_t sm[];
   const int N = f.N;
   const int lines = f.lines();
   const int64_t pix = f.pix();
   constexpr int C = CC;  // coils (one warp each), a compile-time stride
-  const int in_f2 = (2 + C) * N;  // float2 of the slab before the scaling row
+  const int nrow = mode == 4 ? 4 : 2;
+  const int in_f2 = (nrow + C) * N;  // float2 of the slab before the scaling row
   float2* tw_s = reinterpret_cast<float2*>(sm);
   uint8_t* reg = reinterpret_cast<uint8_t*>(tw_s + G);
   float2* row0 = reinterpret_cast<float2*>(reg);
   float2* row1 = row0 + N;
-  float2* maps = row1 + N;
+  float2* row2 = row1 + N;
+  float2* row3 = row2 + N;
+  float2* maps = row0 + nrow * N;
   const float* srow = reinterpret_cast<const float*>(reg + in_f2 * 8);
   float2* scr = reinterpret_cast<float2*>(reg);
   float2* out_s = reinterpret_cast<float2*>(reg);  // [G][C+1]
-  __shared__ double red[33];
+  __shared__ double red[99];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto issue = [&](int i0) {
     const size_t off = static_cast<size_t>(i0) * N;
     if (mode >= 1) {
       cp_async_bytes(row0, r + off, N * 8);
-      if (mode == 1 && iter > 0) cp_async_bytes(row1, p + off, N * 8);
+      if ((mode == 1 && iter > 0) || mode == 4) cp_async_bytes(row1, p + off, N * 8);
+      if (mode == 4) {
+        cp_async_bytes(row2, ap + off, N * 8);
+        cp_async_bytes(row3, xs + off, N * 8);
+      }
     } else if (f.smaps) {
       cp_async_bytes(row0, x + off, N * 8);
     }
@@ -508,7 +533,24 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
   // the first item (and the twiddles) stream in while the panel scale is reduced
   cp_async_bytes(tw_s, f.tw, G * 8);
   if (blockIdx.x < lines) issue(blockIdx.x);
-  const double total = sum_partials(parts, nparts, red);
+  double total, alpha = 0.0;
+  if (mode == 4) {  // finish iteration iter-1 (the cg_update scalars)
+    const double3 s3 = sum_partials3(parts, nparts, lines, red);
+    const double rho = st->rho[iter - 1];
+    const bool ok = isfinite(s3.x) && s3.x > 0.0;
+    alpha = ok ? rho / s3.x : 0.0;
+    total = fmax(rho - 2.0 * alpha * s3.y + alpha * alpha * s3.z, 0.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->pap[iter - 1] = s3.x;
+      st->alpha[iter - 1] = alpha;
+      if (!ok) st->curvature_ok = 0;
+      if (!isfinite(s3.x)) st->finite_ok = 0;
+      st->completed = iter;
+    }
+  } else {
+    total = sum_partials(parts, nparts, red);
+  }
+  const float af = static_cast<float>(alpha);
   float sigma;
   double beta = 0.0;
   if (mode == 0) {
@@ -537,13 +579,21 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
     __syncthreads();
     if (mode >= 1) {  // p = r + beta p (p = r at iteration 0 and after a restart); row0 becomes p
       for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const size_t px = static_cast<size_t>(i0) * N + i;
         float2 pv = row0[i];
-        if (mode == 1 && iter > 0) {
+        if (mode == 4) {  // x += alpha p, r -= alpha Ap (the previous iteration's update)
+          const float2 po = row1[i], av = row2[i], xv = row3[i];
+          pv.x -= af * av.x;
+          pv.y -= af * av.y;
+          r[px] = pv;
+          xs[px] = make_float2(xv.x + af * po.x, xv.y + af * po.y);
+        }
+        if ((mode == 1 && iter > 0) || mode == 4) {
           const float2 po = row1[i];
           pv = make_float2(pv.x + bf * po.x, pv.y + bf * po.y);
         }
         row0[i] = pv;
-        p[static_cast<size_t>(i0) * N + i] = pv;
+        p[px] = pv;
       }
       __syncthreads();
     }
@@ -876,6 +926,8 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_mid_kernel(FftArgs f, 
 // per-warp FFT scratch and the coil images [C][N] | (epi_smem) the epilogue inputs of the
 // row, fetched in the slab's copy group: maps [C][N] (with smaps), p row [N] (mode 2),
 // scaling row [N] float. Without epi_smem the epilogue reads them from global memory.
+// Mode 2 with r given also writes Re <r, Ap> and <Ap, Ap> per line into parts[lines + i0] and
+// parts[2 lines + i0], for the next forward rows to finish the CG update (mode 4 there).
 // Reference: ifft512_rows8_regular_crop_scale (nufft_custom_fft_forward_bench.cu:1517-1552)
 // followed by sense_combine_scaled (nufft_fp16x2_cg_bench.cu:27-54).
 template <int G, int CC>
@@ -895,7 +947,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
   float2* emaps = reinterpret_cast<float2*>(reg + region);
   float2* eprow = emaps + (f.smaps ? C * N : 0);
   float* escale = reinterpret_cast<float*>(eprow + (mode >= 2 ? N : 0));
-  __shared__ double red[33];
+  __shared__ double red[99];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto issue = [&](int i0) {
     float2* dst = reinterpret_cast<float2*>(reg);
@@ -946,7 +998,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
       if (i1 < N) img_s[c * N + i1] = v[m];
     }
     __syncthreads();
-    double dot = 0.0;
+    double dot = 0.0, dot_r = 0.0, dot_a = 0.0;
     for (int i1 = threadIdx.x; i1 < N; i1 += blockDim.x) {
       const size_t pix = static_cast<size_t>(i0) * N + i1;
       const float d = (epi_smem ? escale[i1] : f.scaling[pix]) * factor;
@@ -973,6 +1025,11 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
         if (mode == 2) {
           out[pix] = acc;
           dot += static_cast<double>(pv.x) * acc.x + static_cast<double>(pv.y) * acc.y;
+          if (r) {
+            const float2 rv = r[pix];
+            dot_r += static_cast<double>(rv.x) * acc.x + static_cast<double>(rv.y) * acc.y;
+            dot_a += static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y;
+          }
         } else {  // reliable residual r = b - M v (b read through x)
           const float2 bv = x[pix];
           const float2 rv = make_float2(bv.x - acc.x, bv.y - acc.y);
@@ -981,7 +1038,14 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
         }
       }
     }
-    if (mode != 0) {
+    if (mode == 2 && r) {
+      const double3 t = block_sum3(dot, dot_r, dot_a, red);
+      if (threadIdx.x == 0) {
+        parts[i0] = t.x;
+        parts[lines + i0] = t.y;
+        parts[2 * static_cast<int64_t>(lines) + i0] = t.z;
+      }
+    } else if (mode != 0) {
       const double t = block_sum(dot, red);
       if (threadIdx.x == 0) parts[i0] = t;
     }
@@ -1061,8 +1125,8 @@ static size_t fft_scratch_bytes(int C) {
   return sizeof(float2) * static_cast<size_t>(C) * FftSmem<G>::SCR;
 }
 template <int G>
-static size_t fwd_rows_region(const FftArgs& f) {
-  const size_t in = static_cast<size_t>(2 + f.C) * f.N * 8 + static_cast<size_t>(f.N) * 4;
+static size_t fwd_rows_region(const FftArgs& f, int mode) {
+  const size_t in = static_cast<size_t>((mode == 4 ? 4 : 2) + f.C) * f.N * 8 + static_cast<size_t>(f.N) * 4;
   const size_t out = sizeof(float2) * static_cast<size_t>(G) * (f.C + 1);
   return align16(std::max({in, out, fft_scratch_bytes<G>(f.C)}));
 }
@@ -1143,15 +1207,16 @@ static int persistent_grid(K k, int threads, size_t smem, int items, int share =
     default: break;                                         \
   }
 
-void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
-                     const double* partials, int nparts, CgState* st, int iter, cudaStream_t s) {
+void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, float2* r,
+                     const double* partials, int nparts, CgState* st, int iter, cudaStream_t s, float2* xs,
+                     const float2* ap) {
   TSN_G_SWITCH(f.G, {
-    const size_t sm = sizeof(float2) * GG + fwd_rows_region<GG>(f);
+    const size_t sm = sizeof(float2) * GG + fwd_rows_region<GG>(f, mode);
     TSN_FFT_C(f.C, {
       auto k = fwd_rows_kernel<GG, CC>;
       ensure_smem(k, sm);
       const int grid = persistent_grid(k, 32 * f.C, sm, f.lines(), f.share);
-      k<<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter);
+      k<<<grid, 32 * f.C, sm, s>>>(f, x, z1, mode, p, r, partials, nparts, st, iter, xs, ap);
     });
   });
 }
@@ -1250,13 +1315,17 @@ void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters
   cg_finish_kernel<<<1, 256, 0, s>>>(nparts, rr_parts, st, iters);
 }
 
-__global__ void reduce_partials_kernel(double* part, int n) {
+// Block b sums section b (part + b * stride, n values) into its first value.
+__global__ void reduce_partials_kernel(double* part, int n, int64_t stride) {
   __shared__ double red[33];
-  const double t = sum_partials(part, n, red);  // every read lands before block_sum's first barrier
-  if (threadIdx.x == 0) part[0] = t;
+  double* sec = part + blockIdx.x * stride;
+  const double t = sum_partials(sec, n, red);  // every read lands before block_sum's first barrier
+  if (threadIdx.x == 0) sec[0] = t;
 }
 
-void launch_reduce_partials(double* part, int n, cudaStream_t s) { reduce_partials_kernel<<<1, 1024, 0, s>>>(part, n); }
+void launch_reduce_partials(double* part, int n, cudaStream_t s, int sections, int64_t stride) {
+  reduce_partials_kernel<<<sections, 1024, 0, s>>>(part, n, stride);
+}
 
 template <class T>
 __global__ void gather_rows_kernel(const T* __restrict__ src, const int32_t* __restrict__ map, int64_t rows, int width,

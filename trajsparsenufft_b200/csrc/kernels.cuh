@@ -136,16 +136,20 @@ void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t
 // mode 0: plain, sigma from norm partials -> state->sigma_x
 // mode 1: CG iteration k: p = r + beta p (p = r at k == 0), rho_k from rr partials
 // mode 2: CG iteration k after a reliable restart: p = r (beta = 0)
-void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, const float2* r,
-                     const double* partials, int nparts, CgState* st, int iter, cudaStream_t s);
+// mode 4: CG iteration k that first finishes iteration k-1 (x += alpha p, r -= alpha Ap, with
+//         alpha and rho_k from the three partial sections [lines] that inv_rows wrote with r)
+void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, float2* r,
+                     const double* partials, int nparts, CgState* st, int iter, cudaStream_t s,
+                     float2* xs = nullptr, const float2* ap = nullptr);
 // forward columns: z1 (z2 for volumes) -> panel [G^dims][4C] in internal rows, FP16 hi | res
 void launch_fwd_cols(const FftArgs& f, const float2* z1, __half* panel, cudaStream_t s);
 // forward middle axis of a volume: z1 [i0][q2][i1][c] -> z2 [q2][q1][i0][c]
 void launch_fwd_mid(const FftArgs& f, const float2* z1, float2* z2, cudaStream_t s);
 // inverse middle axis of a volume: z2 [q2][q1][i0][c] -> z1 [q2][i0][i1][c] (crop)
 void launch_inv_mid(const FftArgs& f, const float2* z2, float2* z1, cudaStream_t s);
-// total of n partials into part[0], one CTA in a fixed order
-void launch_reduce_partials(double* part, int n, cudaStream_t s);
+// totals of `sections` runs of n partials (stride apart) into each run's first value, one CTA
+// per run in a fixed order
+void launch_reduce_partials(double* part, int n, cudaStream_t s, int sections = 1, int64_t stride = 0);
 // samples [C][M] (scaled by sigma_y, density) -> sample panel [M][4C]
 void launch_split_samples(const float2* y, const float* density, int64_t m, int c, __half* panel,
                           const double* partials, int nparts, CgState* st, cudaStream_t s);
@@ -154,7 +158,8 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
 // inverse rows + crop + deapod + coil combine
 // mode 0: plain adjoint (factor 1/sigma_y): out = [N][N] (smaps) or [C][N][N]
 // mode 1: CG RHS: r = b, x = 0, rr partials
-// mode 2: CG iteration k: ap = factor*AHAp + lambda p, pap partials
+// mode 2: CG iteration k: ap = factor*AHAp + lambda p, pap partials (with r given, also
+//         Re <r, ap> and <ap, ap> partials at partials + lines and + 2 lines)
 // mode 3: reliable residual: out = x - (factor*AHAp + lambda p) with x = the right-hand
 //         side b, p = the iterate and factor from the plain forward's sigma_x; rr partials
 void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r,

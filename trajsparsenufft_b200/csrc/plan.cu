@@ -405,10 +405,10 @@ void allocate_workspaces(tsn_plan* P) {
   P->p.alloc(sizeof(float2) * pix);
   P->ap.alloc(sizeof(float2) * pix);
   P->rhs.alloc(sizeof(float2) * pix);
-  // one partial per line, plus one slot: stage profiling of volumes writes partials at +1 so
-  // the solve's totals in slot 0 stay readable
-  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(lines + 1, kNormParts));
-  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(lines + 1, kNormParts));
+  // three sections of one partial per line (pAp, Re r.Ap, Ap.Ap), plus one slot: stage
+  // profiling of volumes writes partials at +1 so the solve's totals in slot 0 stay readable
+  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(3 * lines + 1, kNormParts));
+  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(3 * lines + 1, kNormParts));
   P->norm_parts.alloc(sizeof(double) * kNormParts);
   P->state.alloc(sizeof(CgState));
   CUDA_OK(cudaMemset(P->state.ptr, 0, sizeof(CgState)));
@@ -443,9 +443,10 @@ FftArgs fft_args(const tsn_plan* P, const void* smaps, int share = 1) {
 
 // Forward FFT chain, image (or coil images) -> grid panel: rows, then (volumes) the middle
 // axis, then the first axis into the panel.
-void fwd_chain(tsn_plan* P, const FftArgs& f, const float2* x, int mode, float2* p, const float2* r,
-               const double* parts, int nparts, CgState* st, int iter, __half* panel, cudaStream_t s) {
-  launch_fwd_rows(f, x, P->z1.as<float2>(), mode, p, r, parts, nparts, st, iter, s);
+void fwd_chain(tsn_plan* P, const FftArgs& f, const float2* x, int mode, float2* p, float2* r,
+               const double* parts, int nparts, CgState* st, int iter, __half* panel, cudaStream_t s,
+               float2* xs = nullptr, const float2* ap = nullptr) {
+  launch_fwd_rows(f, x, P->z1.as<float2>(), mode, p, r, parts, nparts, st, iter, s, xs, ap);
   if (P->dims == 3) {
     launch_fwd_mid(f, P->z1.as<float2>(), P->z2.as<float2>(), s);
     launch_fwd_cols(f, P->z2.as<float2>(), panel, s);
@@ -465,10 +466,12 @@ void inv_to_lines(tsn_plan* P, const FftArgs& f, const float2* grid, cudaStream_
 }
 
 // Partials written per image line are summed once for volumes (N^2 of them would be re-read
-// by every CTA of the next stage); returns how many partials the consumer reads.
-int settle_partials(const tsn_plan* P, double* parts, cudaStream_t s) {
+// by every CTA of the next stage); returns how many partials the consumer reads. `sections`
+// runs of partials, one line count apart, are summed in one launch.
+int settle_partials(const tsn_plan* P, double* parts, cudaStream_t s, int sections = 1) {
   if (P->dims != 3) return P->N;
-  launch_reduce_partials(parts, static_cast<int>(image_pixels(P) / P->N), s);
+  const int64_t lines = image_pixels(P) / P->N;
+  launch_reduce_partials(parts, static_cast<int>(lines), s, sections, lines);
   return 1;
 }
 
@@ -886,9 +889,16 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
   int n_rr = settle_partials(P, rr, s);
   if (reliable_period > 0)  // keep b for the reliable residuals
     CUDA_OK(cudaMemcpyAsync(P->rhs.ptr, R, P->rhs.bytes, cudaMemcpyDeviceToDevice, s));
-  bool restart = false;
+  // An iteration followed by a plain one leaves its x / r update to the next forward rows
+  // (mode 4), which read alpha and rho from three partial sections of the inverse rows; the
+  // last iteration and those before a reliable residual run cg_update.
+  bool restart = false, fused = false;
+  int n_pap = 0;
   for (int k = 0; k < iters; ++k) {
-    fwd_chain(P, f, nullptr, restart ? 2 : 1, Pv, R, rr, n_rr, st, k, P->panel.as<__half>(), s);
+    if (fused)
+      fwd_chain(P, f, nullptr, 4, Pv, R, pap, n_pap, st, k, P->panel.as<__half>(), s, X, AP);
+    else
+      fwd_chain(P, f, nullptr, restart ? 2 : 1, Pv, R, rr, n_rr, st, k, P->panel.as<__half>(), s);
     restart = false;
     InterpOut of;
     of.panel = P->spanel.as<__half>();
@@ -902,11 +912,14 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     oa.coils = P->C;
     launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
     inv_to_lines(P, f, P->grid.as<float2>(), s);
-    launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, pap, st, k, inv_s2, lam, s);
-    const int n_pap = settle_partials(P, pap, s);
+    const bool reliable = reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters;
+    fused = k + 1 < iters && !reliable;
+    launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, fused ? R : nullptr, Pv, pap, st, k, inv_s2, lam, s);
+    n_pap = settle_partials(P, pap, s, fused ? 3 : 1);
+    if (fused) continue;
     launch_cg_update(P->N, lines, n_pap, X, R, Pv, AP, pap, rr, st, k, s);
     n_rr = settle_partials(P, rr, s);
-    if (reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters) {
+    if (reliable) {
       // r = b - (A^H W A + lambda) x: plain forward of x, then the adjoint into residual mode
       launch_norm_partials(X, image_pixels(P), P->norm_parts.as<double>(), s);
       fwd_chain(P, f, X, 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, P->panel.as<__half>(), s);
@@ -1196,10 +1209,15 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
     CgState* st = plan->state.as<CgState>();
     float2 *X = xbuf.as<float2>(), *R = plan->r.as<float2>(), *Pv = plan->p.as<float2>(), *AP = plan->ap.as<float2>();
     double *pap = plan->parts_pap.as<double>(), *rr = plan->parts_rr.as<double>();
-    // iteration index 1 keeps p = r + beta p live; the stages read state written by the solve
+    // iteration index 1 keeps p = r + beta p live; the stages read state written by the solve.
+    // The row stages run as in the solve's inner iterations: forward rows finishing the
+    // previous update (mode 4), inverse rows writing the three partial sections; x, r and p
+    // drift over the repetitions, and only the times are kept.
     auto stage = [&](int which) {
       switch (which) {
-        case TSN_STAGE_FWD_ROWS: launch_fwd_rows(f, nullptr, plan->z1.as<float2>(), 1, Pv, R, rr, nparts, st, 1, s); break;
+        case TSN_STAGE_FWD_ROWS:
+          launch_fwd_rows(f, nullptr, plan->z1.as<float2>(), 4, Pv, R, pap, nparts, st, 1, s, X, AP);
+          break;
         case TSN_STAGE_FWD_COLS: launch_fwd_cols(f, z_cols, plan->panel.as<__half>(), s); break;
         case TSN_STAGE_FWD_MID:
           if (vol) launch_fwd_mid(f, plan->z1.as<float2>(), plan->z2.as<float2>(), s);
@@ -1224,7 +1242,7 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
         case TSN_STAGE_INV_COLS: launch_inv_cols(f, plan->grid.as<float2>(), z_cols, s); break;
         case TSN_STAGE_INV_ROWS:
           // volumes: partials stay per line here; cg_update below reads the solve's total
-          launch_inv_rows(f, plan->z1.as<float2>(), AP, 2, nullptr, nullptr, Pv, vol ? rr + 1 : pap, st, 1, 1.0f,
+          launch_inv_rows(f, plan->z1.as<float2>(), AP, 2, nullptr, R, Pv, vol ? rr + 1 : pap, st, 1, 1.0f,
                           1e-4f, s);
           break;
         default: launch_cg_update(plan->N, f.lines(), nparts, X, R, Pv, AP, pap, vol ? rr + 1 : rr, st, 1, s); break;
