@@ -273,20 +273,23 @@ tsn_status tsn_fft_adjoint_image_static(int32_t im_size, int32_t grid_size, int3
 
 /* ---- stage timing (autotuner and roofline reporting) ---------------------------------- */
 enum {
-  TSN_STAGE_FWD_ROWS = 0,   /* forward FFT x-stage (SENSE, deapodization, padding)          */
+  TSN_STAGE_FWD_ROWS = 0,   /* forward FFT x-stage (SENSE, deapodization, padding; in CG    *
+                             * iterations after the first, the previous x, r update)       */
   TSN_STAGE_FWD_COLS = 1,   /* forward FFT y-stage -> FP16 hi|res grid panel                 */
   TSN_STAGE_INTERP_FWD = 2, /* sparse G interpolation -> FP16 hi|res sample panel            */
   TSN_STAGE_INTERP_ADJ = 3, /* sparse G^H gather -> grid                                     */
   TSN_STAGE_INV_COLS = 4,   /* inverse FFT first stage                                       */
   TSN_STAGE_INV_ROWS = 5,   /* inverse FFT second stage + crop + deapod + coil combine      */
-  TSN_STAGE_CG_UPDATE = 6,  /* x, r updates + FP64 partial dots                              */
+  TSN_STAGE_CG_UPDATE = 6,  /* x, r update + FP64 partial dots (after the last iteration)    */
   TSN_STAGE_FWD_MID = 7,    /* volumes: forward FFT over the middle axis (0 ms for images)   */
   TSN_STAGE_INV_MID = 8,    /* volumes: inverse FFT over the middle axis (0 ms for images)   */
   TSN_STAGE_COUNT = 9
 };
 /* Runs one CG-SENSE solve of `iters` iterations to populate the workspaces, then times each
  * stage of a CG iteration `reps` times in isolation with CUDA events on `stream` and writes
- * the mean milliseconds per launch to stage_ms[TSN_STAGE_COUNT] (synchronizes). */
+ * the mean milliseconds per launch to stage_ms[TSN_STAGE_COUNT] (synchronizes). The row
+ * stages are timed in the form the inner iterations run (forward rows with the previous
+ * update, inverse rows with its partials); the plan's solve state is left overwritten. */
 tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, int32_t reps,
                               double* stage_ms, tsn_stream_t stream);
 
