@@ -1,0 +1,63 @@
+"""The device CG's scalar schedule, restated on the host, against the oracle's CG.
+
+The GPU solve finishes iteration k-1's update inside iteration k's forward rows: the inverse
+rows write per-line FP64 partials of <p, Ap>, Re <r, Ap> and <Ap, Ap>, and the next forward
+rows take alpha = rho / <p, Ap> and rho' = rho - 2 alpha Re <r, Ap> + alpha^2 <Ap, Ap> before
+x += alpha p, r -= alpha Ap, p = r + beta p. Only the last iteration (and one before a
+reliable residual) computes rho' directly from r. This restatement keeps the device's
+precisions (FP32 vectors, FP64 per-line partials summed in order) and must track the oracle's
+CG (oracle/operator.py:cg_sense, reference_sparse_solver.py:297-323) on a small system.
+"""
+import numpy as np
+
+from oracle import operator as oop
+
+
+def _line_dots(a, b, n):
+    """FP64 per-line partials of Re <a, b> over lines of n values, summed in line order."""
+    prod = (a.real.astype(np.float64) * b.real + a.imag.astype(np.float64) * b.imag).reshape(-1, n)
+    return float(np.sum(prod.sum(axis=1)))
+
+
+def _fused_cg(normal, b, iters, n):
+    x = np.zeros_like(b)
+    r = b.copy()
+    p = r.copy()
+    rho = _line_dots(r, r, n)
+    hist = [rho]
+    for k in range(iters):
+        ap = normal(p).astype(np.complex64)
+        pap = _line_dots(p, ap, n)
+        alpha = rho / pap if pap > 0 else 0.0
+        af = np.float32(alpha)
+        if k + 1 < iters:  # finished by the next forward rows
+            rap, apap = _line_dots(r, ap, n), _line_dots(ap, ap, n)
+            rho_new = max(rho - 2.0 * alpha * rap + alpha * alpha * apap, 0.0)
+            x = (x + af * p).astype(np.complex64)
+            r = (r - af * ap).astype(np.complex64)
+            beta = np.float32(rho_new / max(rho, 1e-30))
+            p = (r + beta * p).astype(np.complex64)
+        else:  # cg_update: direct residual norm
+            x = (x + af * p).astype(np.complex64)
+            r = (r - af * ap).astype(np.complex64)
+            rho_new = _line_dots(r, r, n)
+        hist.append(rho_new)
+        rho = rho_new
+    return x, hist
+
+
+def test_fused_update_tracks_the_oracle_cg():
+    rng = np.random.default_rng(20260823)
+    n, m, lam = 16, 600, 1e-2
+    a = (rng.standard_normal((m, n * n)) + 1j * rng.standard_normal((m, n * n))) / np.sqrt(m)
+    y = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    normal = (lambda v: a.conj().T @ (a @ v) + lam * v)
+    b = (a.conj().T @ y).astype(np.complex64)
+    iters = 10
+    x_ref, res_ref, status = oop.cg_sense(lambda v: a @ v, lambda v: a.conj().T @ v, y, iters, lam)
+    assert status["completed_iterations"] == iters
+    x, hist = _fused_cg(normal, b, iters, n)
+    # residual history: the expansion form agrees with the direct one to FP32 vector rounding
+    np.testing.assert_allclose(np.sqrt(hist), res_ref, rtol=2e-4)
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-4
+    assert hist[-1] < 1e-2 * hist[0]
