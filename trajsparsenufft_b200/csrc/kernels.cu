@@ -484,7 +484,7 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
 // Mode 4 also finishes CG iteration iter-1, which then needs no cg_update launch: parts holds
 // three sections [lines] of <p, Ap>, Re <r, Ap> and <Ap, Ap> from the inverse rows, so
 // alpha = rho / pAp, and rho' = |r - alpha Ap|^2 = rho - 2 alpha Re <r, Ap> + alpha^2 <Ap, Ap>
-// (FP64); each row updates x += alpha p and r -= alpha Ap before p = r + beta p.
+// (FP64, a negative rounding residue clamped to 0); each row updates x += alpha p and r -= alpha Ap before p = r + beta p.
 // Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844);
 // the CG update of reference_sparse_solver.py:297-323.
 template <int G, int CC>
@@ -539,12 +539,13 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
     const double rho = st->rho[iter - 1];
     const bool ok = isfinite(s3.x) && s3.x > 0.0;
     alpha = ok ? rho / s3.x : 0.0;
-    total = fmax(rho - 2.0 * alpha * s3.y + alpha * alpha * s3.z, 0.0);
+    const double rn = rho - 2.0 * alpha * s3.y + alpha * alpha * s3.z;
+    total = rn < 0.0 ? 0.0 : rn;  // a negative rounding residue clamps to 0; NaN stays NaN
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       st->pap[iter - 1] = s3.x;
       st->alpha[iter - 1] = alpha;
       if (!ok) st->curvature_ok = 0;
-      if (!isfinite(s3.x)) st->finite_ok = 0;
+      if (!isfinite(s3.x) || !isfinite(total)) st->finite_ok = 0;
       st->completed = iter;
     }
   } else {
