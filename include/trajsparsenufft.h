@@ -258,15 +258,18 @@ tsn_status tsn_fft_adjoint_image(tsn_plan* plan, const void* grid_c64, const voi
                                  tsn_stream_t stream);
 
 /* No counterpart in the reference.  The adjoint FFT endpoint for callers that cannot call
- * cudaMalloc (code running under CUDA graph capture, hosts whose device allocator is frozen
- * after start-up, services that reserve all device memory up front): no plan, every input
- * and output from the caller, the one intermediate in a fixed device array of
- * grid_size * im_size * coils <= 1 Mi complex values (8 MiB, enough for 512 x 256 x 8);
- * larger shapes return TSN_ERR_SHAPE.  Computes the same as tsn_fft_adjoint_image
- * (grid[G*G][C] c64 with rows q1*G + q0; centered != 0 when the image is centred on the grid,
- * as in trajectory plans without TSN_FLAG_REFERENCE_LAYOUT).  The first call on a device sets
- * up the arrays (make it before any stream capture); every call in the process shares them,
- * so calls that overlap on the GPU race and must be ordered by the caller.  Allocates nothing. */
+ * cudaMalloc (hosts whose device allocator is frozen after start-up, services that reserve
+ * all device memory up front, plug-ins inside an application that owns the device memory):
+ * no plan, every input and output from the caller, the one intermediate in a fixed device
+ * array of grid_size * im_size * coils <= 1 Mi complex values (8 MiB, enough for
+ * 512 x 256 x 8); larger shapes return TSN_ERR_SHAPE.  Computes the same as
+ * tsn_fft_adjoint_image (grid[G*G][C] c64 with rows q1*G + q0; centered != 0 when the image
+ * is centred on the grid, as in trajectory plans without TSN_FLAG_REFERENCE_LAYOUT).  The
+ * first call on a device sets up the device that is current at that call: it looks up the
+ * arrays' device addresses and fills the twiddle tables of every supported grid size, so
+ * make it before any stream capture.  Later calls write only the scratch array and the
+ * output; every call in the process shares the scratch array, so calls that overlap on the
+ * GPU race and must be ordered by the caller.  Allocates nothing. */
 tsn_status tsn_fft_adjoint_image_static(int32_t im_size, int32_t grid_size, int32_t coils,
                                         int32_t centered, const void* grid_c64, const void* smaps,
                                         const float* scaling, void* x, tsn_stream_t stream);

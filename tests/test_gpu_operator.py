@@ -139,12 +139,16 @@ def test_cg_sense_headline_matches_fp64_kb():
 
 def test_cg_curvature_failure_is_reported_not_trapped():
     """A negative Tikhonov weight makes the normal operator indefinite: the status word
-    reports the non-positive curvature; nothing traps."""
+    reports the non-positive curvature and the iteration count stops before the failing
+    iteration (0 here: the first denominator is already negative), as the reference solver
+    stops there (reference_sparse_solver.py:281-287); nothing traps."""
     plan = _plan("small")
     _, st, yt = torch_inputs("small")
-    x, hist, status = plan.cg_sense(yt, st, lam=-1e12, iters=3)
-    assert status["positive_curvature"] is False
-    assert status.get("failure") == "CURVATURE"
+    for iters in (1, 3):
+        x, hist, status = plan.cg_sense(yt, st, lam=-1e12, iters=iters)
+        assert status["positive_curvature"] is False
+        assert status.get("failure") == "CURVATURE"
+        assert status["completed_iterations"] == 0, status
 
 
 def test_misaligned_device_arrays_are_rejected():
@@ -181,6 +185,25 @@ def test_long_cg_stays_on_the_fp64_path(iters):
     nd = onudft.Nudft(traj, n)
     x_ref, _, _ = oracle_cg(lambda v: nd.forward(v, s), lambda v: nd.adjoint(v, s), measurement(name), w, iters, 1e-4)
     assert oop.magnitude_nrmse(x_gpu.cpu().numpy(), x_ref) <= 2e-3
+
+
+def test_fused_update_residual_matches_the_direct_norm():
+    """The fused CG update takes rho' from an expansion over the stored r and Ap; the last
+    iteration of a solve sums |r|^2 directly instead.  A solve of k iterations therefore ends
+    on the direct norm of r_k, and a solve of k + 1 iterations reaches r_k through the
+    expansion: the two residuals agree to FP32 rounding late into the solve (rtol 1e-3 on
+    |r|), because each expansion restarts from the direct <r, r> of the previous iteration."""
+    name = "cfg0"
+    traj, x, s, n, g, c, j, readout = case(name)
+    plan = _plan(name)
+    _, st, yt = torch_inputs(name)
+    from trajsparsenufft_b200 import synth
+    w = torch.from_numpy(synth.ramp_density(traj, readout)).cuda()
+    for k in (10, 30):
+        _, hist_k, _ = plan.cg_sense(yt, st, density=w, lam=1e-4, iters=k)
+        _, hist_k1, _ = plan.cg_sense(yt, st, density=w, lam=1e-4, iters=k + 1)
+        assert hist_k[-1] < 1e-2 * hist_k[0]
+        np.testing.assert_allclose(hist_k1[:k + 1], hist_k[:k + 1], rtol=1e-3)
 
 
 def _oracle_reliable_cg(fwd, adj, y, w, iters, lam, period, direction):

@@ -143,6 +143,32 @@ __device__ __forceinline__ double3 block_sum3(double a, double b, double c, doub
   return t;
 }
 
+// Four deterministic block sums at once; `scratch` holds 132 doubles.
+__device__ __forceinline__ double4 block_sum4(double a, double b, double c, double d, double* scratch) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  c = warp_sum(c);
+  d = warp_sum(d);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    scratch[warp] = a;
+    scratch[33 + warp] = b;
+    scratch[66 + warp] = c;
+    scratch[99 + warp] = d;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += scratch[33 * threadIdx.x + w];
+    scratch[33 * threadIdx.x + 32] = t;
+  }
+  __syncthreads();
+  const double4 t = make_double4(scratch[32], scratch[65], scratch[98], scratch[131]);
+  __syncthreads();
+  return t;
+}
+
 // Power-of-two scale bringing rms to ~target (FP16 rounding commutes with it).
 __device__ __forceinline__ float pow2_scale(double sum_sq, double count, float target) {
   const double rms = sqrt(sum_sq / count);

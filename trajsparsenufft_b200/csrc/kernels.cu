@@ -421,15 +421,16 @@ __device__ __forceinline__ double sum_partials(const double* part, int nparts, d
   return block_sum(a, scratch);
 }
 
-// Sums of three partial sections [nparts] spaced `stride` apart, as sum_partials does each.
-__device__ __forceinline__ double3 sum_partials3(const double* part, int nparts, int64_t stride, double* scratch) {
-  double a = 0.0, b = 0.0, c = 0.0;
+// Sums of four partial sections [nparts] spaced `stride` apart, as sum_partials does each.
+__device__ __forceinline__ double4 sum_partials4(const double* part, int nparts, int64_t stride, double* scratch) {
+  double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
     a += part[i];
     b += part[stride + i];
     c += part[2 * stride + i];
+    d += part[3 * stride + i];
   }
-  return block_sum3(a, b, c, scratch);
+  return block_sum4(a, b, c, d, scratch);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -482,9 +483,12 @@ __device__ __forceinline__ void cp_async_slab(float2* dst, const float2* src, in
 //     mode 4 (CG, fused update): row0 = r, row1 = p, row2 = A p, row3 = x rows, maps = S_c rows
 //   the per-warp FFT scratch [C][SCR], and the output rows [G][C+1] float2.
 // Mode 4 also finishes CG iteration iter-1, which then needs no cg_update launch: parts holds
-// three sections [lines] of <p, Ap>, Re <r, Ap> and <Ap, Ap> from the inverse rows, so
-// alpha = rho / pAp, and rho' = |r - alpha Ap|^2 = rho - 2 alpha Re <r, Ap> + alpha^2 <Ap, Ap>
-// (FP64, a negative rounding residue clamped to 0); each row updates x += alpha p and r -= alpha Ap before p = r + beta p.
+// four sections [lines] of <p, Ap>, Re <r, Ap>, <Ap, Ap> and <r, r> from the inverse rows, so
+// rho = <r, r> (a direct sum over the stored r, as the reference's rs_old), alpha = rho / pAp,
+// and rho' = |r - alpha Ap|^2 = rho - 2 alpha Re <r, Ap> + alpha^2 <Ap, Ap> (FP64, a negative
+// rounding residue clamped to 0).  The expansion restarts from the direct sum every
+// iteration, so its rounding does not accumulate while rho falls.  Each row updates
+// x += alpha p and r -= alpha Ap before p = r + beta p.
 // Reference: fft512_rows4_shared16_pad_scale<true> (nufft_custom_fft_forward_bench.cu:1600-1844);
 // the CG update of reference_sparse_solver.py:297-323.
 template <int G, int CC>
@@ -511,7 +515,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
   const float* srow = reinterpret_cast<const float*>(reg + in_f2 * 8);
   float2* scr = reinterpret_cast<float2*>(reg);
   float2* out_s = reinterpret_cast<float2*>(reg);  // [G][C+1]
-  __shared__ double red[99];
+  __shared__ double red[132];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto issue = [&](int i0) {
     const size_t off = static_cast<size_t>(i0) * N;
@@ -535,18 +539,23 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
   if (blockIdx.x < lines) issue(blockIdx.x);
   double total, alpha = 0.0;
   if (mode == 4) {  // finish iteration iter-1 (the cg_update scalars)
-    const double3 s3 = sum_partials3(parts, nparts, lines, red);
-    const double rho = st->rho[iter - 1];
+    const double4 s3 = sum_partials4(parts, nparts, lines, red);
+    const double rho = s3.w;  // |r_{iter-1}|^2 summed directly
     const bool ok = isfinite(s3.x) && s3.x > 0.0;
     alpha = ok ? rho / s3.x : 0.0;
     const double rn = rho - 2.0 * alpha * s3.y + alpha * alpha * s3.z;
     total = rn < 0.0 ? 0.0 : rn;  // a negative rounding residue clamps to 0; NaN stays NaN
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->rho[iter - 1] = rho;  // the history keeps the direct sum
       st->pap[iter - 1] = s3.x;
       st->alpha[iter - 1] = alpha;
+      // the iteration count stops at the first failing iteration, as the reference solver
+      // stops there (reference_sparse_solver.py:281-293); the solve itself runs on with alpha 0
+      const bool fin = isfinite(s3.x) && isfinite(rho) && isfinite(total);
+      const bool prior_ok = st->curvature_ok && st->finite_ok;
       if (!ok) st->curvature_ok = 0;
-      if (!isfinite(s3.x) || !isfinite(total)) st->finite_ok = 0;
-      st->completed = iter;
+      if (!fin) st->finite_ok = 0;
+      if (prior_ok && ok && fin) st->completed = iter;
     }
   } else {
     total = sum_partials(parts, nparts, red);
@@ -927,8 +936,9 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_mid_kernel(FftArgs f, 
 // per-warp FFT scratch and the coil images [C][N] | (epi_smem) the epilogue inputs of the
 // row, fetched in the slab's copy group: maps [C][N] (with smaps), p row [N] (mode 2),
 // scaling row [N] float. Without epi_smem the epilogue reads them from global memory.
-// Mode 2 with r given also writes Re <r, Ap> and <Ap, Ap> per line into parts[lines + i0] and
-// parts[2 lines + i0], for the next forward rows to finish the CG update (mode 4 there).
+// Mode 2 with r given also writes Re <r, Ap>, <Ap, Ap> and <r, r> per line into
+// parts[lines + i0], parts[2 lines + i0] and parts[3 lines + i0], for the next forward rows to
+// finish the CG update (mode 4 there).
 // Reference: ifft512_rows8_regular_crop_scale (nufft_custom_fft_forward_bench.cu:1517-1552)
 // followed by sense_combine_scaled (nufft_fp16x2_cg_bench.cu:27-54).
 template <int G, int CC>
@@ -948,7 +958,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
   float2* emaps = reinterpret_cast<float2*>(reg + region);
   float2* eprow = emaps + (f.smaps ? C * N : 0);
   float* escale = reinterpret_cast<float*>(eprow + (mode >= 2 ? N : 0));
-  __shared__ double red[99];
+  __shared__ double red[132];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto issue = [&](int i0) {
     float2* dst = reinterpret_cast<float2*>(reg);
@@ -999,7 +1009,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
       if (i1 < N) img_s[c * N + i1] = v[m];
     }
     __syncthreads();
-    double dot = 0.0, dot_r = 0.0, dot_a = 0.0;
+    double dot = 0.0, dot_r = 0.0, dot_a = 0.0, dot_rr = 0.0;
     for (int i1 = threadIdx.x; i1 < N; i1 += blockDim.x) {
       const size_t pix = static_cast<size_t>(i0) * N + i1;
       const float d = (epi_smem ? escale[i1] : f.scaling[pix]) * factor;
@@ -1030,6 +1040,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
             const float2 rv = r[pix];
             dot_r += static_cast<double>(rv.x) * acc.x + static_cast<double>(rv.y) * acc.y;
             dot_a += static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y;
+            dot_rr += static_cast<double>(rv.x) * rv.x + static_cast<double>(rv.y) * rv.y;
           }
         } else {  // reliable residual r = b - M v (b read through x)
           const float2 bv = x[pix];
@@ -1040,11 +1051,12 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
       }
     }
     if (mode == 2 && r) {
-      const double3 t = block_sum3(dot, dot_r, dot_a, red);
+      const double4 t = block_sum4(dot, dot_r, dot_a, dot_rr, red);
       if (threadIdx.x == 0) {
         parts[i0] = t.x;
         parts[lines + i0] = t.y;
         parts[2 * static_cast<int64_t>(lines) + i0] = t.z;
+        parts[3 * static_cast<int64_t>(lines) + i0] = t.w;
       }
     } else if (mode != 0) {
       const double t = block_sum(dot, red);
@@ -1081,9 +1093,10 @@ __global__ void cg_update_kernel(int N, int nparts, float2* __restrict__ x, floa
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->pap[iter] = pap;
     st->alpha[iter] = alpha;
+    const bool prior_ok = st->curvature_ok && st->finite_ok;  // completed stops at a failure
     if (!ok) st->curvature_ok = 0;
     if (!isfinite(pap)) st->finite_ok = 0;
-    st->completed = iter + 1;
+    if (prior_ok && ok) st->completed = iter + 1;
   }
   const float af = static_cast<float>(alpha);
   double acc = 0.0;
@@ -1110,7 +1123,10 @@ __global__ void cg_finish_kernel(int nparts, const double* __restrict__ rr_parts
   const double rho = sum_partials(rr_parts, nparts, red);
   if (threadIdx.x == 0) {
     st->rho[iters] = rho;
-    if (!isfinite(rho)) st->finite_ok = 0;
+    if (!isfinite(rho)) {  // a non-finite last update: the last iteration did not complete
+      if (st->curvature_ok && st->finite_ok && st->completed == iters) st->completed = iters - 1;
+      st->finite_ok = 0;
+    }
   }
 }
 

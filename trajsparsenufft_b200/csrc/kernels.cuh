@@ -137,7 +137,8 @@ void launch_norm_partials(const float2* v, int64_t n, double* part, cudaStream_t
 // mode 1: CG iteration k: p = r + beta p (p = r at k == 0), rho_k from rr partials
 // mode 2: CG iteration k after a reliable restart: p = r (beta = 0)
 // mode 4: CG iteration k that first finishes iteration k-1 (x += alpha p, r -= alpha Ap, with
-//         alpha and rho_k from the three partial sections [lines] that inv_rows wrote with r)
+//         alpha, rho_{k-1} and rho_k from the four partial sections [lines] that inv_rows
+//         wrote with r)
 void launch_fwd_rows(const FftArgs& f, const float2* x, float2* z1, int mode, float2* p, float2* r,
                      const double* partials, int nparts, CgState* st, int iter, cudaStream_t s,
                      float2* xs = nullptr, const float2* ap = nullptr);
@@ -159,7 +160,7 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
 // mode 0: plain adjoint (factor 1/sigma_y): out = [N][N] (smaps) or [C][N][N]
 // mode 1: CG RHS: r = b, x = 0, rr partials
 // mode 2: CG iteration k: ap = factor*AHAp + lambda p, pap partials (with r given, also
-//         Re <r, ap> and <ap, ap> partials at partials + lines and + 2 lines)
+//         Re <r, ap>, <ap, ap> and <r, r> partials at partials + lines, + 2 lines, + 3 lines)
 // mode 3: reliable residual: out = x - (factor*AHAp + lambda p) with x = the right-hand
 //         side b, p = the iterate and factor from the plain forward's sigma_x; rr partials
 void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r,

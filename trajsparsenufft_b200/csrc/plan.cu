@@ -405,10 +405,10 @@ void allocate_workspaces(tsn_plan* P) {
   P->p.alloc(sizeof(float2) * pix);
   P->ap.alloc(sizeof(float2) * pix);
   P->rhs.alloc(sizeof(float2) * pix);
-  // three sections of one partial per line (pAp, Re r.Ap, Ap.Ap), plus one slot: stage
+  // four sections of one partial per line (pAp, Re r.Ap, Ap.Ap, r.r), plus one slot: stage
   // profiling of volumes writes partials at +1 so the solve's totals in slot 0 stay readable
-  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(3 * lines + 1, kNormParts));
-  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(3 * lines + 1, kNormParts));
+  P->parts_pap.alloc(sizeof(double) * std::max<int64_t>(4 * lines + 1, kNormParts));
+  P->parts_rr.alloc(sizeof(double) * std::max<int64_t>(4 * lines + 1, kNormParts));
   P->norm_parts.alloc(sizeof(double) * kNormParts);
   P->state.alloc(sizeof(CgState));
   CUDA_OK(cudaMemset(P->state.ptr, 0, sizeof(CgState)));
@@ -890,7 +890,7 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
   if (reliable_period > 0)  // keep b for the reliable residuals
     CUDA_OK(cudaMemcpyAsync(P->rhs.ptr, R, P->rhs.bytes, cudaMemcpyDeviceToDevice, s));
   // An iteration followed by a plain one leaves its x / r update to the next forward rows
-  // (mode 4), which read alpha and rho from three partial sections of the inverse rows; the
+  // (mode 4), which read alpha and rho from four partial sections of the inverse rows; the
   // last iteration and those before a reliable residual run cg_update.
   bool restart = false, fused = false;
   int n_pap = 0;
@@ -915,7 +915,7 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     const bool reliable = reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters;
     fused = k + 1 < iters && !reliable;
     launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, fused ? R : nullptr, Pv, pap, st, k, inv_s2, lam, s);
-    n_pap = settle_partials(P, pap, s, fused ? 3 : 1);
+    n_pap = settle_partials(P, pap, s, fused ? 4 : 1);
     if (fused) continue;
     launch_cg_update(P->N, lines, n_pap, X, R, Pv, AP, pap, rr, st, k, s);
     n_rr = settle_partials(P, rr, s);
@@ -1211,7 +1211,7 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
     double *pap = plan->parts_pap.as<double>(), *rr = plan->parts_rr.as<double>();
     // iteration index 1 keeps p = r + beta p live; the stages read state written by the solve.
     // The row stages run as in the solve's inner iterations: forward rows finishing the
-    // previous update (mode 4), inverse rows writing the three partial sections; x, r and p
+    // previous update (mode 4), inverse rows writing the four partial sections; x, r and p
     // drift over the repetitions, and only the times are kept.
     auto stage = [&](int which) {
       switch (which) {
