@@ -1,9 +1,12 @@
 #!/usr/bin/env python3
 """Generate the committed golden pack fixtures by running the reference itself.
 
-Run in a container where the reference repository is mounted (default
-/root/reference, override with TSN_REFERENCE_ROOT).  The GPU box never runs
-this script; tests read only the files it writes next to it.
+Run in a container where the reference repository is checked out, naming its root:
+
+    python tests/golden/make_golden.py --reference-root <path of the reference checkout>
+
+(or set TSN_REFERENCE_ROOT).  The GPU box never runs this script; tests read only the
+files it writes next to it.
 
 Fixtures
 --------
@@ -27,6 +30,8 @@ prod_*/
 
 from __future__ import annotations
 
+import argparse
+import importlib
 import json
 import os
 import shutil
@@ -41,20 +46,25 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REFERENCE = Path(os.environ.get("TSN_REFERENCE_ROOT", "/root/reference"))
-
 sys.path.insert(0, str(REPO))
-sys.path.insert(0, str(REFERENCE))
-# export_torchkbnufft_gpu_case imports torchkbnufft at module load but its
-# planner functions never call it.
-sys.modules.setdefault("torchkbnufft", types.ModuleType("torchkbnufft"))
-
-from src import nufft_layout_oracle as ref_oracle  # noqa: E402
-from src import export_gpu_case as ref_export  # noqa: E402
-from src import export_torchkbnufft_gpu_case as ref_prod  # noqa: E402
 
 from oracle import kb  # noqa: E402
 from trajsparsenufft_b200 import synth  # noqa: E402
+
+# the reference's modules, bound by load_reference()
+ref_oracle = ref_export = ref_prod = None
+
+
+def load_reference(root: Path) -> None:
+    """Import the reference's src/ modules from the checkout at `root`."""
+    global ref_oracle, ref_export, ref_prod
+    sys.path.insert(0, str(root))
+    # export_torchkbnufft_gpu_case imports torchkbnufft at module load but its
+    # planner functions never call it.
+    sys.modules.setdefault("torchkbnufft", types.ModuleType("torchkbnufft"))
+    ref_oracle = importlib.import_module("src.nufft_layout_oracle")
+    ref_export = importlib.import_module("src.export_gpu_case")
+    ref_prod = importlib.import_module("src.export_torchkbnufft_gpu_case")
 
 
 def csr_of(view) -> dict:
@@ -183,9 +193,17 @@ def make_production(name: str, trajectory: np.ndarray, im_size: int, grid: int, 
 
 
 def main() -> int:
-    if not (REFERENCE / "src" / "nufft_layout_oracle.py").is_file():
-        print(f"reference not found at {REFERENCE}", file=sys.stderr)
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference-root", default=os.environ.get("TSN_REFERENCE_ROOT"),
+                    help="root of the reference checkout (or TSN_REFERENCE_ROOT)")
+    args = ap.parse_args()
+    if not args.reference_root:
+        ap.error("name the reference checkout with --reference-root or TSN_REFERENCE_ROOT")
+    root = Path(args.reference_root)
+    if not (root / "src" / "nufft_layout_oracle.py").is_file():
+        print(f"reference not found at {root}", file=sys.stderr)
         return 2
+    load_reference(root)
     make_layout_packs()
     make_exports()
     small = synth.golden_radial(16, 32)
