@@ -22,6 +22,8 @@ def case(name: str):
         n, g, c, spokes, readout = 128, 256, 4, 96, 256
     elif name == "headline":      # 256^2, 8 coils, 256 x 512 golden-angle radial
         n, g, c, spokes, readout = 256, 512, 8, 256, 512
+    elif name == "grad4":         # one case of the differentiable config: 4x-undersampled radial
+        n, g, c, spokes, readout = 256, 512, 8, 128, 512
     elif name == "c16":
         n, g, c, spokes, readout = 128, 256, 16, 64, 256
     elif name == "n192":          # grid 384 = 3 x 128: radix-3 FFT step
@@ -50,16 +52,10 @@ def oracle_cg(forward, adjoint, y, density, iters, lam):
 
 @functools.lru_cache(maxsize=None)
 def measurement(name: str):
-    """FP64 NUDFT k-space + 1e-3 rms complex noise (BASELINE config 0 recipe)."""
+    """FP64 direct NUDFT k-space + 1e-3 rms complex noise (the config 0 recipe; the headline's
+    131072 x 65536 x 8 NUDFT takes a few seconds as chunked GEMMs)."""
     traj, x, s, n, *_ = case(name)
-    if name == "headline":
-        # exact NUDFT at 131072 x 65536 x 8 is minutes on CPU; an FP64 KB NUFFT with
-        # J = 6 is within 3e-6 of it (checked at cfg0 in test_oracle_accuracy) and is
-        # used for data generation only
-        op = oop.KbSenseOperator(traj, n, 2 * n, 6, workers=8)
-        y = op.forward(x, s)
-    else:
-        y = onudft.Nudft(traj, n).forward(x, s)
+    y = onudft.Nudft(traj, n).forward(x, s)
     return synth.add_noise(y, SEED)
 
 

@@ -51,11 +51,14 @@ def _oracle_loss(ops, y, s, x0, xt):
     return float(np.sum(np.abs(x - xt) ** 2))
 
 
-def test_unrolled_cg_gradients_match_fp64_finite_differences():
+def _fd_check(name, directions):
+    """Hand-written gradients of the unrolled CG on the FP16x2 GPU plan against FP64 central
+    finite differences of the same unrolled CG on the FP64 KB oracle, along `directions`
+    random directions cycling over (y, maps, x0)."""
     from trajsparsenufft_b200 import autograd as tad
     from trajsparsenufft_b200.operator import Plan
-    traj, x, s, n, g, c, j, _ = case("small")
-    y = measurement("small").astype(np.complex128)
+    traj, x, s, n, g, c, j, _ = case(name)
+    y = measurement(name).astype(np.complex128)
     rng = np.random.default_rng(17)
     x0 = 0.1 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
     plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=j)
@@ -67,11 +70,11 @@ def test_unrolled_cg_gradients_match_fp64_finite_differences():
     loss.backward()
     grads = [t.grad.cpu().numpy().astype(np.complex128) for t in leaves]
 
-    oops = _OracleOps(oop.KbSenseOperator(traj, n, g, j, workers=8), n)
+    oops = _OracleOps(oop.KbSenseOperator(traj, n, g, j, workers=16), n)
     base = [y, s.astype(np.complex128), x0]
     assert abs(float(loss.detach()) - _oracle_loss(oops, *base, x)) <= 1e-3 * float(loss.detach())
     got, want = [], []
-    for k in range(32):
+    for k in range(directions):
         v = k % 3
         d = rng.standard_normal(base[v].shape) + 1j * rng.standard_normal(base[v].shape)
         eps = 1e-6 * np.linalg.norm(base[v]) / np.linalg.norm(d)
@@ -84,6 +87,21 @@ def test_unrolled_cg_gradients_match_fp64_finite_differences():
         want.append(fd)
     got, want = np.array(got), np.array(want)
     assert np.linalg.norm(got - want) <= 1e-3 * np.linalg.norm(want)
+    for v in range(3):  # each input's directional derivatives on their own
+        sel = np.arange(v, directions, 3)
+        assert np.linalg.norm(got[sel] - want[sel]) <= 1e-3 * np.linalg.norm(want[sel]), v
+
+
+def test_unrolled_cg_gradients_match_fp64_finite_differences():
+    """64^2 image, 4 coils: 32 directions."""
+    _fd_check("small", 32)
+
+
+def test_unrolled_cg_gradients_match_fp64_finite_differences_grad4_shape():
+    """One case of the differentiable configuration (256^2 image, 512^2 grid, 8 coils,
+    golden-angle radial 128 x 512, 10 iterations, checkpoint every 2): 9 directions, three per
+    input, since every FP64 oracle evaluation is a full 10-iteration CG at this size."""
+    _fd_check("grad4", 9)
 
 
 def test_differentiable_forward_matches_graph_solver():

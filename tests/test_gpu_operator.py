@@ -86,6 +86,32 @@ def test_forward_adjoint_match_oracle(name, layout):
     assert gap <= 1e-5
 
 
+def test_headline_operator_accuracy():
+    """The headline shape (256^2 image, 512^2 grid, 8 coils, 131072 samples, J = 6) through the
+    product's default plan: forward and adjoint against the FP16x2 emulation (<= 2e-5), the FP64
+    KB operator (<= 5e-4) and the FP64 direct NUDFT (forward on every 64th sample, adjoint in
+    full; <= 5e-4), and the adjointness gap of the FP16x2 pair (<= 1e-5)."""
+    traj, x, s, n, g, c, j, _ = case("headline")
+    plan = _plan("headline")
+    xt, st, _ = torch_inputs("headline")
+    emu = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16", panel_mode="split2", workers=8)
+    f64 = oop.KbSenseOperator(traj, n, g, j, workers=8)
+    y_gpu = plan.forward(xt, st).cpu().numpy()
+    assert rel_l2(y_gpu, emu.forward(x, s)) <= 2e-5
+    assert rel_l2(y_gpu, f64.forward(x, s)) <= 5e-4
+    sub = np.arange(0, len(traj), 64)
+    assert rel_l2(y_gpu[:, sub], onudft.Nudft(traj[sub], n).forward(x, s)) <= 5e-4
+    rng = np.random.default_rng(12)
+    yr = (rng.standard_normal((c, len(traj))) + 1j * rng.standard_normal((c, len(traj)))).astype(np.complex64)
+    a_gpu = plan.adjoint(torch.from_numpy(yr).cuda(), st).cpu().numpy()
+    assert rel_l2(a_gpu, emu.adjoint(yr, s)) <= 2e-5
+    assert rel_l2(a_gpu, f64.adjoint(yr, s)) <= 5e-4
+    assert rel_l2(a_gpu, onudft.Nudft(traj, n).adjoint(yr, s)) <= 5e-4
+    left = np.vdot(y_gpu.astype(np.complex128), yr)
+    right = np.vdot(x.astype(np.complex128), a_gpu)
+    assert abs(left - right) / (np.linalg.norm(yr) * np.linalg.norm(y_gpu)) <= 1e-5
+
+
 def test_pack_dirs_drop_in_matches_trajectory_plan(tmp_path):
     """Reference-format directories (written by our planner) load as a drop-in and give
     bit-identical results to the in-memory reference-layout plan."""
@@ -126,6 +152,8 @@ def test_cg_sense_cfg0_matches_fp64_nudft(name):
 
 
 def test_cg_sense_headline_matches_fp64_kb():
+    """Headline CG-SENSE (k-space from the direct FP64 NUDFT plus noise) against the FP64 KB
+    CG on the same data: magnitude NRMSE within the 0.2% gate."""
     traj, x, s, n, g, c, j, _ = case("headline")
     plan = _plan("headline")
     xt, st, yt = torch_inputs("headline")
@@ -135,6 +163,32 @@ def test_cg_sense_headline_matches_fp64_kb():
     y = measurement("headline")
     x_ref, res_ref, _ = oracle_cg(lambda v: op.forward(v, s), lambda v: op.adjoint(v, s), y, None, 10, 1e-4)
     assert oop.magnitude_nrmse(x_gpu.cpu().numpy(), x_ref) <= 2e-3
+
+
+@pytest.mark.parametrize("layout", ["reference", "centered"])
+def test_cg_sense_matches_the_reference_solver_output(layout):
+    """The GPU CG-SENSE against what the reference's own reference_sparse_solver computed
+    (tests/golden/solver_small.npz, fp16x2 variant: FP16 matrix, FP16 high + residual panels,
+    10 iterations; the fixture's power-of-two rescaling undone).  With the reference's complex
+    pack layout the coefficients round to FP16 exactly as there: image within 2e-4 rel and
+    residual history within 2e-3.  The centred real pack rounds different coefficients
+    (the phase moved into the FFT): magnitude NRMSE within the 0.2% gate."""
+    from golden_io import GOLDEN
+    from trajsparsenufft_b200.operator import Plan
+    d = np.load(GOLDEN / "solver_small.npz")
+    n, g, c, j, iters = (int(v) for v in d["shape"])
+    a, k = int(d["fp16x2_maps_scale_exp"]), int(d["fp16x2_data_scale_exp"])
+    want = d["x_fp16x2"] * 2.0 ** (a - k)
+    plan = Plan.from_trajectory(d["trajectory"], im_size=n, grid_size=g, coils=c, width=j,
+                                reference_layout=(layout == "reference"))
+    x_gpu, hist, status = plan.cg_sense(torch.from_numpy(d["data"]).cuda(), torch.from_numpy(d["smaps"]).cuda(),
+                                        lam=float(d["lam"]), iters=iters)
+    assert status["positive_curvature"] and status["finite"] and status["completed_iterations"] == iters
+    x_gpu = x_gpu.cpu().numpy()
+    assert oop.magnitude_nrmse(x_gpu, want) <= 2e-3
+    if layout == "reference":
+        assert rel_l2(x_gpu, want) <= 2e-4
+        np.testing.assert_allclose(hist, d["residuals_fp16x2"] * 2.0 ** -(a + k), rtol=2e-3)
 
 
 def test_cg_curvature_failure_is_reported_not_trapped():
