@@ -537,10 +537,11 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
   // the first item (and the twiddles) stream in while the panel scale is reduced
   cp_async_bytes(tw_s, f.tw, G * 8);
   if (blockIdx.x < lines) issue(blockIdx.x);
-  double total, alpha = 0.0;
+  double total, alpha = 0.0, rho_prev = 0.0;
   if (mode == 4) {  // finish iteration iter-1 (the cg_update scalars)
     const double4 s3 = sum_partials4(parts, nparts, lines, red);
     const double rho = s3.w;  // |r_{iter-1}|^2 summed directly
+    rho_prev = rho;
     const bool ok = isfinite(s3.x) && s3.x > 0.0;
     alpha = ok ? rho / s3.x : 0.0;
     const double rn = rho - 2.0 * alpha * s3.y + alpha * alpha * s3.z;
@@ -568,7 +569,9 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) fwd_rows_kernel(FftArgs f,
     if (blockIdx.x == 0 && threadIdx.x == 0) st->sigma_x = sigma;
   } else {
     sigma = pow2_scale(total, static_cast<double>(pix), kPanelTarget);
-    beta = (iter == 0 || mode == 2) ? 0.0 : total / fmax(st->rho[iter - 1], 1e-30);
+    // mode 4 divides by its own direct rho (block 0 rewrites st->rho[iter - 1] concurrently)
+    const double rho_old = mode == 4 ? rho_prev : (iter > 0 ? st->rho[iter - 1] : 1.0);
+    beta = (iter == 0 || mode == 2) ? 0.0 : total / fmax(rho_old, 1e-30);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       st->rho[iter] = total;
       st->beta[iter] = beta;
@@ -1067,7 +1070,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
 
 constexpr int kCgRowPix = 4;  // pixels per thread of cg_update: rows up to 1024 pixels at 256 threads
 
-__global__ void cg_update_kernel(int N, int nparts, float2* __restrict__ x, float2* __restrict__ r,
+__global__ void cg_update_kernel(int N, int nparts, int lines, float2* __restrict__ x, float2* __restrict__ r,
                                  const float2* __restrict__ p, const float2* __restrict__ ap,
                                  const double* __restrict__ pap_parts, double* __restrict__ rr_parts,
                                  CgState* __restrict__ st, int iter) {
@@ -1086,11 +1089,14 @@ __global__ void cg_update_kernel(int N, int nparts, float2* __restrict__ x, floa
       rv[j] = r[pix];
     }
   }
+  // <p, Ap> and the direct <r, r> of the r this iteration started from (sections 0 and 3 of
+  // the inverse rows' partials)
   const double pap = sum_partials(pap_parts, nparts, red);
-  const double rho = st->rho[iter];
+  const double rho = sum_partials(pap_parts + 3 * static_cast<int64_t>(lines), nparts, red);
   const bool ok = isfinite(pap) && pap > 0.0;
   const double alpha = ok ? rho / pap : 0.0;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->rho[iter] = rho;
     st->pap[iter] = pap;
     st->alpha[iter] = alpha;
     const bool prior_ok = st->curvature_ok && st->finite_ok;  // completed stops at a failure
@@ -1325,7 +1331,7 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
 
 void launch_cg_update(int N, int lines, int nparts, float2* x, float2* r, const float2* p, const float2* ap,
                       const double* pap_parts, double* rr_parts, CgState* st, int iter, cudaStream_t s) {
-  cg_update_kernel<<<lines, 256, 0, s>>>(N, nparts, x, r, p, ap, pap_parts, rr_parts, st, iter);
+  cg_update_kernel<<<lines, 256, 0, s>>>(N, nparts, lines, x, r, p, ap, pap_parts, rr_parts, st, iter);
 }
 
 void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters, cudaStream_t s) {

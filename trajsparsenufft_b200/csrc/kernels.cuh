@@ -167,7 +167,8 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
                      const float2* p, double* partials, CgState* st, int iter, float inv_scale2,
                      float lambda_scaled, cudaStream_t s);
 // CG update over `lines` lines of N pixels: x += alpha p, r -= alpha ap, one rr partial per
-// line; alpha from the first `nparts` pAp partials
+// line; alpha = <r, r> / <p, Ap> from the first `nparts` partials of sections 3 and 0 of the
+// inverse rows' four partial sections (`lines` apart)
 void launch_cg_update(int N, int lines, int nparts, float2* x, float2* r, const float2* p, const float2* ap,
                       const double* pap_parts, double* rr_parts, CgState* st, int iter, cudaStream_t s);
 void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters, cudaStream_t s);

@@ -914,8 +914,8 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     inv_to_lines(P, f, P->grid.as<float2>(), s);
     const bool reliable = reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters;
     fused = k + 1 < iters && !reliable;
-    launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, fused ? R : nullptr, Pv, pap, st, k, inv_s2, lam, s);
-    n_pap = settle_partials(P, pap, s, fused ? 4 : 1);
+    launch_inv_rows(f, P->z1.as<float2>(), AP, 2, nullptr, R, Pv, pap, st, k, inv_s2, lam, s);
+    n_pap = settle_partials(P, pap, s, 4);
     if (fused) continue;
     launch_cg_update(P->N, lines, n_pap, X, R, Pv, AP, pap, rr, st, k, s);
     n_rr = settle_partials(P, rr, s);
