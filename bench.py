@@ -213,7 +213,7 @@ def run_ours(args, cfg) -> dict:
     seed = 20260823 + rank
     traj, x_np, s_np, w_np = synth_inputs(cfg, seed)
     plan = Plan.from_trajectory(traj, im_size=cfg["n"], grid_size=cfg["g"], coils=cfg["c"], width=cfg["width"],
-                                device=local)
+                                device=local, interp=args.interp)
     x_true = torch.from_numpy(x_np).to(dev)
     smaps = torch.from_numpy(s_np).to(dev)
     density = None if w_np is None else torch.from_numpy(w_np).to(dev)
@@ -347,6 +347,7 @@ def run_ours(args, cfg) -> dict:
         "config": {"workload": workload_text(cfg), "samples_per_coil": plan.samples, "recons_per_step": 1,
                    "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
                    "planner": "optimized/morton split24", "pack": "real KB coefficients, centred image",
+                   "interp_kernel": plan.interp,
                    "tiles": plan.info["tiles"], "groups": plan.info["groups"]},
         "e2e": {"value": round(e2e_value, 3), "unit": "recons/s",
                 "h2d_bytes_per_step": int(y.numel() * 8 + smaps.numel() * 8),
@@ -1002,6 +1003,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", choices=tuple(CONFIGS), default="headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--interp", choices=("auto", "mma_sp", "tcgen05"), default="auto",
+                    help="sparse interpolation kernel of the plans (headline configuration)")
     ap.add_argument("--streams", type=int, default=0, help="batch48: concurrent case streams (default 4)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -62,9 +62,13 @@ enum { TSN_POLICY_TRAJECTORY = 0, TSN_POLICY_MORTON = 1, TSN_POLICY_OVERLAP = 2,
 enum { TSN_ILLEGAL_SPLIT24 = 0, TSN_ILLEGAL_CSR_RESIDUAL = 1 };
 /* Views. */
 enum { TSN_VIEW_G = 0, TSN_VIEW_GT = 1 };
-/* Interpolation kernel choice.  The pack's 16-row groups each carry their own K32 column
- * set (M_TILE = 16, src/nufft_layout_oracle.py:29); tcgen05.mma needs 64 or 128 rows sharing
- * one K operand, so TSN_INTERP_TCGEN05 is reserved and refused with TSN_ERR_UNSUPPORTED. */
+/* Interpolation kernel choice (the reference runs warp mma.sp m16n8k32 per 16-row tile,
+ * nufft_spmma_bench.cu:402-663).  TSN_INTERP_MMA_SP: the same instruction family, one warp per
+ * tile stream.  TSN_INTERP_TCGEN05: tcgen05.mma.sp with seven 16-row tiles stacked into one
+ * M = 128 operand, B rows gathered by TMA, accumulators in tensor memory; built for the
+ * real-coefficient pack (trajectory plans without TSN_FLAG_REFERENCE_LAYOUT) with 8 coils,
+ * refused with TSN_ERR_UNSUPPORTED otherwise.  TSN_INTERP_AUTO picks the faster one measured
+ * for the shape. */
 enum { TSN_INTERP_AUTO = 0, TSN_INTERP_MMA_SP = 1, TSN_INTERP_TCGEN05 = 2 };
 /* Plan flags. */
 enum {
@@ -99,16 +103,18 @@ typedef struct tsn_plan_info {
   int64_t pack_bytes[2];      /* device bytes of each view's pack              */
   int64_t workspace_bytes;    /* device workspace owned by the plan            */
   double plan_seconds;        /* host planner wall time                        */
-  int32_t interp;             /* kernel actually used (TSN_INTERP_MMA_SP)              */
+  int32_t interp;             /* kernel actually used (TSN_INTERP_MMA_SP or _TCGEN05)   */
   int32_t dims;               /* 2 or 3                                                 */
-  int32_t reserved[6];
+  int32_t device_error;       /* nonzero once a tcgen05 launch of this plan gave up a bounded
+                                 wait (read at call time: synchronize the plan's streams first) */
+  int32_t reserved[5];
 } tsn_plan_info;
 
 typedef struct tsn_cg_status {
   int32_t completed_iterations;
   int32_t positive_curvature;  /* 1 unless a denominator was <= 0 or non-finite   */
   int32_t finite;              /* 1 unless the solution / residual went non-finite */
-  int32_t timeout;
+  int32_t timeout;             /* 1 when a bounded device wait of the solve gave up */
   double residual0, residual_final;
 } tsn_cg_status;
 

@@ -57,7 +57,8 @@ class PlanInfo(C.Structure):
         ("kernel_width", C.c_int32), ("components", C.c_int32),
         ("groups", C.c_int64 * 2), ("tiles", C.c_int64 * 2), ("active_rows", C.c_int64 * 2),
         ("nnz", C.c_int64 * 2), ("pack_bytes", C.c_int64 * 2), ("workspace_bytes", C.c_int64),
-        ("plan_seconds", C.c_double), ("interp", C.c_int32), ("dims", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("plan_seconds", C.c_double), ("interp", C.c_int32), ("dims", C.c_int32), ("device_error", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

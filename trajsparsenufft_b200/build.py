@@ -23,7 +23,7 @@ OUT = PKG / "_build"
 LIB = PKG / "libtrajsparsenufft.so"
 
 HOST_SOURCES = ["planner.cpp", "kb.cpp", "pack_io.cpp", "api_host.cpp"]
-CUDA_SOURCES = ["kernels.cu", "plan.cu", "noalloc.cu"]
+CUDA_SOURCES = ["kernels.cu", "plan.cu", "noalloc.cu", "interp_tc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

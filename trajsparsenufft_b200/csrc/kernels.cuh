@@ -119,6 +119,39 @@ inline bool fft_grid_supported(int g) {
 
 void launch_interp(const InterpView& v, const __half* panel, int rowh, bool split, int epi, bool conj,
                    const InterpOut& o, cudaStream_t s);
+
+// ---- interpolation on tcgen05.mma.sp (real pack, 8 coils) ------------------------------------
+// Seven 16-row tiles are stacked into one M = 128 sparse A operand (rows 112..127 zero) and
+// their 32 gathered panel rows side by side into one N = 7 x 32 = 224 B operand; one
+// tcgen05.mma.sp (K = 32) per step, of which each tile keeps its diagonal 16 x 32 block.  The
+// record stream is cut into steps of seven slot records:
+//   [0, 3584)        A of slots 0..6: 512 B each, the canonical K-major layout without swizzle
+//                    (rows 0-7 k-chunk 0 | rows 0-7 chunk 1 | rows 8-15 chunk 0 | chunk 1,
+//                    8 rows x 16 B each)
+//   [3584 + 256 j)   slot j: int32 gather row per column (-1: dead column or idle slot),
+//                    [+128) u32 sparse metadata in tensor-memory lane order,
+//                    [+192) RecordInfo (flags 0: idle slot), [+208) 24-bit output rows
+constexpr int kTcSlots = 7;
+constexpr int kTcSlotABytes = 512;
+constexpr int kTcSlotInfoBytes = 256;
+constexpr int kTcStepABytes = kTcSlots * kTcSlotABytes;                          // 3584
+constexpr int kTcStepBytes = kTcStepABytes + kTcSlots * kTcSlotInfoBytes;        // 5376
+constexpr int kTcPartialFloats = 32 * 16;  // one split-group chunk: 32 columns x 16 rows
+
+struct InterpTcView {
+  const uint8_t* steps = nullptr;      // step blocks, grouped by CTA
+  const int2* cta_steps = nullptr;     // per CTA: [first step, end step)
+  int32_t* counters = nullptr;         // one per split group, zero between launches
+  float* partials = nullptr;           // [chunk slots][kTcPartialFloats]
+  int32_t* error = nullptr;            // nonzero after a bounded wait gave up
+  int32_t n_ctas = 0;
+};
+// whether the tensor-core interpolation is built for this view shape
+inline bool interp_tc_supported(int rowh, int ncomp) { return rowh == 32 && ncomp == 1; }
+// epi: EPI_SAMPLES, EPI_GRID or EPI_PANEL; panel: the [rows][32] f16 panel the view gathers
+void launch_interp_tc(const InterpTcView& v, const __half* panel, int epi, const InterpOut& o, cudaStream_t s);
+// shared memory of one CTA of the tensor-core interpolation
+size_t interp_tc_smem_bytes();
 // warps the persistent interpolation kernel keeps resident on this device for a panel row
 // width / component count (used to cut the item list into per-warp runs)
 int interp_resident_warps(int rowh, int ncomp, int stages);

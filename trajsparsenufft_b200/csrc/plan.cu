@@ -75,6 +75,10 @@ struct HostView {
 struct DevView {
   DeviceBuffer records, counters, partials, ranges;
   InterpView v;
+  // tcgen05 step stream (when the plan runs this view on the tensor-memory kernel)
+  DeviceBuffer tc_steps, tc_ranges, tc_counters, tc_partials;
+  InterpTcView tc;
+  bool use_tc = false;
   // warp runs cut for a 1/share slice of the GPU (batched cases run side by side)
   std::vector<int64_t> item_ends;  // record position after each work item, stream order
   DeviceBuffer ranges_shared;
@@ -105,6 +109,8 @@ std::vector<int> g_const_devices;
 struct tsn_plan {
   tsn_plan_desc desc{};
   int N = 0, G = 0, C = 0, J = 0, ncomp = 0, shift = 0, rowh = 0;
+  bool use_tc = false;    // interpolation on tcgen05.mma.sp (TSN_INTERP_TCGEN05)
+  DeviceBuffer tc_error;  // int32, set by a tensor-core launch whose bounded wait gave up
   int dims = 2;  // 2: [N][N] images on a G^2 grid; 3: [N][N][N] volumes on a G^3 grid
   int64_t M = 0;
   DevView view[2];
@@ -218,6 +224,134 @@ std::vector<int2> cut_ranges(const std::vector<int64_t>& item_ends, int64_t tile
 
 constexpr int64_t kLocalityPanelBytes = 64ll << 20;  // about half of the 126 MB L2
 
+int device_sm_count() {
+  int dev = 0, sms = 0;
+  CUDA_OK(cudaGetDevice(&dev));
+  CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return std::max(1, sms);
+}
+
+// tcgen05 step stream of one real-pack view (layout in kernels.cuh).  Work items are the
+// view's row groups, cut into chunks of at most kTcChunkTiles tiles (longer than the warp
+// kernel's: every split chunk publishes its partial sums through a fence and an atomic, which
+// here stalls a whole CTA pipeline rather than one warp).  The items, in row-group order, are
+// cut into one contiguous run per CTA (one CTA per SM) with balanced tile counts; inside a CTA
+// the items go longest first to the slot that frees first (lowest slot on ties), each item's
+// tiles on consecutive steps.  Column ids keep the warp records' dead-column marking (-1); A
+// is re-laid into the canonical K-major layout and the pair metadata into tensor-memory lane
+// order (lane l of a tile holds pair word 2 (l % 8) + l / 8: the lower or upper 16 metadata
+// bits of rows l % 8 and l % 8 + 8).
+constexpr uint32_t kTcChunkTiles = 32;
+
+void build_tc_steps(tsn_plan* P, DevView& d, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
+  const int64_t tiles = h.tiles(), groups = h.groups();
+  struct Item {
+    int32_t group;
+    uint32_t t0, t1;
+    int32_t split, first_slot, chunk, nchunks;
+  };
+  std::vector<Item> items;
+  std::vector<int64_t> ends;
+  int32_t slots = 0, nsplit = 0;
+  int64_t pos = 0;
+  for (int64_t g = 0; g < groups; ++g) {
+    const uint32_t a = h.group_offsets[g], b = h.group_offsets[g + 1];
+    if (a == b) continue;
+    const int32_t nch = static_cast<int32_t>((b - a + kTcChunkTiles - 1) / kTcChunkTiles);
+    const uint32_t len = (b - a + nch - 1) / nch;  // balanced chunk lengths
+    for (int32_t k = 0; k < nch; ++k) {
+      const uint32_t t0 = a + k * len, t1 = std::min<uint32_t>(b, a + (k + 1) * len);
+      items.push_back(Item{static_cast<int32_t>(g), t0, t1, nch > 1 ? nsplit : -1, slots, k, nch});
+      pos += t1 - t0;
+      ends.push_back(pos);
+    }
+    if (nch > 1) {
+      slots += nch;
+      ++nsplit;
+    }
+  }
+  if (pos != tiles) fail(TSN_ERR_FORMAT, "group offsets do not cover the tiles");
+  const int ctas = device_sm_count();
+  const std::vector<int2> runs = cut_ranges(ends, tiles, ctas);
+  struct Place { size_t item; int32_t slot, step; };
+  std::vector<std::vector<Place>> per_cta(runs.size());
+  std::vector<int2> cta_steps(runs.size());
+  size_t it = 0;
+  int64_t total_steps = 0;
+  for (size_t c = 0; c < runs.size(); ++c) {
+    std::vector<size_t> mine;
+    while (it < ends.size() && ends[it] <= runs[c].y) mine.push_back(it++);
+    std::stable_sort(mine.begin(), mine.end(), [&](size_t x, size_t y) {
+      return items[x].t1 - items[x].t0 > items[y].t1 - items[y].t0;
+    });
+    int32_t free_at[kTcSlots] = {0};
+    for (size_t m : mine) {
+      const int slot = static_cast<int>(std::min_element(free_at, free_at + kTcSlots) - free_at);
+      per_cta[c].push_back(Place{m, slot, free_at[slot]});
+      free_at[slot] += static_cast<int32_t>(items[m].t1 - items[m].t0);
+    }
+    const int32_t steps = *std::max_element(free_at, free_at + kTcSlots);
+    cta_steps[c] = make_int2(static_cast<int>(total_steps), static_cast<int>(total_steps + steps));
+    total_steps += steps;
+  }
+  if (it != ends.size()) fail(TSN_ERR_FORMAT, "tensor-core step schedule lost work items");
+  std::vector<uint8_t> steps(static_cast<size_t>(std::max<int64_t>(total_steps, 1)) * kTcStepBytes, 0);
+  // idle slots: every column dead (the gathers read nothing), flags 0 (nothing accumulates)
+  for (int64_t st = 0; st < total_steps; ++st)
+    for (int j = 0; j < kTcSlots; ++j)
+      std::memset(steps.data() + st * kTcStepBytes + kTcStepABytes + j * kTcSlotInfoBytes, 0xFF, 128);
+  for (size_t c = 0; c < runs.size(); ++c)
+    for (const Place& pl : per_cta[c]) {
+      const Item& itm = items[pl.item];
+      int32_t live_rows = 0;
+      uint8_t rows24[48];
+      for (int s = 0; s < kMTile; ++s) {
+        const int32_t v = h.group_row_ids[static_cast<size_t>(itm.group) * kMTile + s];
+        if (v >= 0) live_rows |= static_cast<int32_t>(1u << (kRecLiveShift + s));
+        const int64_t row = v < 0 ? kRecRowPad : (rows_are_cells ? to_internal(P, v) : v);
+        for (int k = 0; k < 3; ++k) rows24[3 * s + k] = static_cast<uint8_t>((row >> (8 * k)) & 0xFF);
+      }
+      for (uint32_t t = itm.t0; t < itm.t1; ++t) {
+        const int64_t step = cta_steps[c].x + pl.step + (t - itm.t0);
+        uint8_t* blk = steps.data() + step * static_cast<int64_t>(kTcStepBytes);
+        uint8_t* a = blk + pl.slot * kTcSlotABytes;
+        for (int row = 0; row < 16; ++row)
+          for (int kc = 0; kc < 16; ++kc)
+            std::memcpy(a + (row % 8) * 16 + (row / 8) * 256 + (kc / 8) * 128 + (kc % 8) * 2,
+                        &h.a[0][static_cast<size_t>(t) * 256 + row * 16 + kc], 2);
+        uint8_t* info = blk + kTcStepABytes + pl.slot * kTcSlotInfoBytes;
+        const uint32_t live = live_columns(h, t);
+        int32_t cols[kKTile];
+        for (int q = 0; q < kKTile; ++q) {
+          int64_t col = h.tile_col_ids[static_cast<size_t>(t) * kKTile + q];
+          if (cols_are_cells) col = to_internal(P, col);
+          cols[q] = ((live >> q) & 1u) ? static_cast<int32_t>(col) : -1;
+        }
+        std::memcpy(info, cols, sizeof cols);
+        uint32_t lanes[16];
+        for (int l = 0; l < 16; ++l) lanes[l] = h.meta[0][static_cast<size_t>(t) * 16 + 2 * (l % 8) + l / 8];
+        std::memcpy(info + 128, lanes, 64);
+        RecordInfo ri;
+        ri.flags = live_rows | (t == itm.t0 ? kRecFirst : 0) | (t + 1 == itm.t1 ? kRecLast : 0);
+        ri.split = itm.split;
+        ri.first_slot = itm.first_slot;
+        ri.chunk = itm.chunk | (itm.nchunks << 16);
+        std::memcpy(info + 192, &ri, sizeof ri);
+        std::memcpy(info + 208, rows24, 48);
+      }
+    }
+  d.tc_counters.upload(std::vector<int32_t>(std::max(nsplit, 1), 0));
+  d.tc_partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kTcPartialFloats);
+  d.tc.counters = d.tc_counters.as<int32_t>();
+  d.tc.partials = d.tc_partials.as<float>();
+  d.tc_steps.upload(steps);
+  d.tc_ranges.upload(cta_steps);
+  d.tc.steps = d.tc_steps.as<uint8_t>();
+  d.tc.cta_steps = d.tc_ranges.as<int2>();
+  d.tc.n_ctas = static_cast<int32_t>(cta_steps.size());
+  d.use_tc = true;
+}
+
 void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
   DevView& d = P->view[which];
   const int64_t tiles = h.tiles(), groups = h.groups();
@@ -324,6 +458,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   }
   if (pos != tiles) fail(TSN_ERR_FORMAT, "group offsets do not cover the tiles");
   const std::vector<int2> ranges = cut_ranges(d.item_ends, tiles, interp_resident_warps(4 * P->C, ncomp, stages));
+  if (P->use_tc) build_tc_steps(P, d, h, rows_are_cells, cols_are_cells);
   d.records.upload(records);
   d.counters.upload(std::vector<int32_t>(std::max(nsplit, 1), 0));
   d.partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kPartialFloats * 32);
@@ -360,8 +495,26 @@ void check_desc(const tsn_plan_desc* d) {
   if (d->im_size <= 0 || d->im_size % 2 || d->grid_size < d->im_size) fail(TSN_ERR_SHAPE, "need an even image size <= grid size");
   if (d->coils < 4 || d->coils > 16 || d->coils % 4) fail(TSN_ERR_UNSUPPORTED, "coil count must be 4, 8, 12 or 16");
   if (d->kernel_width < 1 || d->kernel_width > 16) fail(TSN_ERR_ARG, "kernel width out of range");
-  if (d->interp != TSN_INTERP_AUTO && d->interp != TSN_INTERP_MMA_SP)
-    fail(TSN_ERR_UNSUPPORTED, "only the mma.sp interpolation kernel is built (16-row pack tiles)");
+  if (d->interp != TSN_INTERP_AUTO && d->interp != TSN_INTERP_MMA_SP && d->interp != TSN_INTERP_TCGEN05)
+    fail(TSN_ERR_ARG, "unknown interpolation kernel");
+}
+
+// Interpolation kernel of a plan: tcgen05.mma.sp when asked for (real-coefficient pack with 8
+// coils only), the warp mma.sp kernel otherwise.
+bool choose_tc(const tsn_plan_desc* d, int ncomp, int coils) {
+  const bool ok = interp_tc_supported(4 * coils, ncomp);
+  if (d->interp == TSN_INTERP_TCGEN05 && !ok)
+    fail(TSN_ERR_UNSUPPORTED,
+         "the tcgen05 interpolation is built for the real-coefficient pack (centred layout) with 8 coils");
+  return d->interp == TSN_INTERP_TCGEN05 && ok;
+}
+
+// Error word of the tensor-core views (after allocate_workspaces).
+void setup_tc(tsn_plan* P) {
+  if (!P->use_tc) return;
+  P->tc_error.upload(std::vector<int32_t>(1, 0));
+  for (DevView& d : P->view)
+    if (d.present && d.use_tc) d.tc.error = P->tc_error.as<int32_t>();
 }
 
 // FFT endpoints are built for power-of-two grids of 128..1024 points.
@@ -658,16 +811,18 @@ tsn_status tsn_plan_create_from_pack(const char* fwd_real, const char* fwd_imag,
       for (size_t i = 0; i < sc.size(); ++i) sc[i] = static_cast<float>(d[i]);
     }
     P->scaling.upload(sc);
+    P->use_tc = choose_tc(desc, P->ncomp, P->C);
     if (fwd_real) upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
     if (adj_real) upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
     allocate_workspaces(P.get());
+    setup_tc(P.get());
     P->info.samples = P->M;
     P->info.im_size = P->N;
     P->info.grid_size = P->G;
     P->info.coils = P->C;
     P->info.kernel_width = P->J;
     P->info.components = P->ncomp;
-    P->info.interp = TSN_INTERP_MMA_SP;
+    P->info.interp = P->use_tc ? TSN_INTERP_TCGEN05 : TSN_INTERP_MMA_SP;
     P->info.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = P.release();
     return TSN_OK;
@@ -729,18 +884,20 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
       CUDA_OK(cudaSetDevice(desc->device));
       P->scaling.upload(sc);
       P->info.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      P->use_tc = choose_tc(desc, P->ncomp, P->C);
       upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
       hv[0] = HostView();
       upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
       hv[1] = HostView();
       allocate_workspaces(P.get());
+      setup_tc(P.get());
       P->info.samples = P->M;
       P->info.im_size = P->N;
       P->info.grid_size = P->G;
       P->info.coils = P->C;
       P->info.kernel_width = P->J;
       P->info.components = P->ncomp;
-      P->info.interp = TSN_INTERP_MMA_SP;
+      P->info.interp = P->use_tc ? TSN_INTERP_TCGEN05 : TSN_INTERP_MMA_SP;
       P->info.dims = 3;
       *out = P.release();
       return TSN_OK;
@@ -773,16 +930,18 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
     CUDA_OK(cudaSetDevice(desc->device));
     P->scaling.upload(sc);
     P->info.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    P->use_tc = choose_tc(desc, P->ncomp, P->C);
     upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
     upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
     allocate_workspaces(P.get());
+    setup_tc(P.get());
     P->info.samples = P->M;
     P->info.im_size = P->N;
     P->info.grid_size = P->G;
     P->info.coils = P->C;
     P->info.kernel_width = P->J;
     P->info.components = P->ncomp;
-    P->info.interp = TSN_INTERP_MMA_SP;
+    P->info.interp = P->use_tc ? TSN_INTERP_TCGEN05 : TSN_INTERP_MMA_SP;
     P->info.dims = 2;
     *out = P.release();
     return TSN_OK;
@@ -803,6 +962,12 @@ tsn_status tsn_plan_get_info(const tsn_plan* plan, tsn_plan_info* info) {
     return TSN_ERR_ARG;
   }
   *info = plan->info;
+  info->device_error = 0;
+  if (plan->use_tc && plan->tc_error.ptr) {
+    cudaSetDevice(plan->desc.device);
+    int32_t err = 0;
+    if (cudaMemcpy(&err, plan->tc_error.ptr, sizeof err, cudaMemcpyDeviceToHost) == cudaSuccess) info->device_error = err;
+  }
   return TSN_OK;
 }
 
@@ -816,6 +981,20 @@ void need_views(const tsn_plan* P, bool fwd, bool adj) {
   CUDA_OK(cudaSetDevice(P->desc.device));
   if ((fwd && !P->view[TSN_VIEW_G].present) || (adj && !P->view[TSN_VIEW_GT].present))
     fail(TSN_ERR_ARG, "plan lacks the pack view this operator needs");
+}
+
+// One interpolation launch of a view: the tensor-core kernel when the plan uses it, else the
+// warp mma.sp kernel (on a 1/share slice of the GPU for batched cases).  The tensor-core
+// kernel always runs its one-CTA-per-SM schedule; batched cases then share SMs as they free.
+void run_interp(const tsn_plan* P, int which, int share, int epi, const InterpOut& o, cudaStream_t s) {
+  const DevView& d = P->view[which];
+  const __half* panel = which == TSN_VIEW_G ? P->panel.as<__half>() : P->spanel.as<__half>();
+  if (d.use_tc) {
+    launch_interp_tc(d.tc, panel, epi, o, s);
+    return;
+  }
+  const InterpView& v = share > 1 ? d.v_shared : d.v;
+  launch_interp(v, panel, P->rowh, true, epi, which == TSN_VIEW_GT, o, s);
 }
 
 void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cudaStream_t s) {
@@ -832,7 +1011,7 @@ void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cud
   o.scale_ptr = &st->sigma_x;
   o.scale_inv = 1;
   o.scale_mul = f.gs();
-  launch_interp(P->view[TSN_VIEW_G].v, P->panel.as<__half>(), P->rowh, true, EPI_SAMPLES, false, o, s);
+  run_interp(P, TSN_VIEW_G, 1, EPI_SAMPLES, o, s);
 }
 
 // Cuts (once per share value, outside any stream capture) the interpolation warp runs for a
@@ -851,11 +1030,6 @@ void prepare_share(tsn_plan* P, int share) {
   }
 }
 
-const InterpView& interp_view(const tsn_plan* P, int which, int share) {
-  const DevView& d = P->view[which];
-  return share > 1 ? d.v_shared : d.v;
-}
-
 void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cudaStream_t s, int share = 1) {
   CgState* st = P->state.as<CgState>();
   launch_norm_partials(static_cast<const float2*>(y), P->M * P->C, P->norm_parts.as<double>(), s);
@@ -865,7 +1039,7 @@ void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cuda
   o.c64 = P->grid.as<float2>();
   o.rows = grid_cells(P);
   o.coils = P->C;
-  launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, o, s);
+  run_interp(P, TSN_VIEW_GT, share, EPI_GRID, o, s);
 }
 
 // The CG-SENSE solve (launch_cg, nufft_fp16x2_cg_bench.cu:241-268). With reliable_period > 0,
@@ -905,12 +1079,12 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     of.density = density;
     of.rows = P->M;
     of.coils = P->C;
-    launch_interp(interp_view(P, TSN_VIEW_G, share), P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
+    run_interp(P, TSN_VIEW_G, share, EPI_PANEL, of, s);
     InterpOut oa;
     oa.c64 = P->grid.as<float2>();
     oa.rows = grid_cells(P);
     oa.coils = P->C;
-    launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
+    run_interp(P, TSN_VIEW_GT, share, EPI_GRID, oa, s);
     inv_to_lines(P, f, P->grid.as<float2>(), s);
     const bool reliable = reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters;
     fused = k + 1 < iters && !reliable;
@@ -923,8 +1097,8 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
       // r = b - (A^H W A + lambda) x: plain forward of x, then the adjoint into residual mode
       launch_norm_partials(X, image_pixels(P), P->norm_parts.as<double>(), s);
       fwd_chain(P, f, X, 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, P->panel.as<__half>(), s);
-      launch_interp(interp_view(P, TSN_VIEW_G, share), P->panel.as<__half>(), P->rowh, true, EPI_PANEL, false, of, s);
-      launch_interp(interp_view(P, TSN_VIEW_GT, share), P->spanel.as<__half>(), P->rowh, true, EPI_GRID, true, oa, s);
+      run_interp(P, TSN_VIEW_G, share, EPI_PANEL, of, s);
+      run_interp(P, TSN_VIEW_GT, share, EPI_GRID, oa, s);
       inv_to_lines(P, f, P->grid.as<float2>(), s);
       launch_inv_rows(f, P->z1.as<float2>(), R, 3, P->rhs.as<float2>(), nullptr, X, rr, st, k, inv_s2, lam, s);
       n_rr = settle_partials(P, rr, s);
@@ -939,7 +1113,9 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
 tsn_status read_cg_state(const tsn_plan* P, int iters, double* residual_history, tsn_cg_status* status,
                          cudaStream_t s) {
   CgState host;
+  int32_t tc_err = 0;
   CUDA_OK(cudaMemcpyAsync(&host, P->state.ptr, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+  if (P->use_tc) CUDA_OK(cudaMemcpyAsync(&tc_err, P->tc_error.ptr, sizeof tc_err, cudaMemcpyDeviceToHost, s));
   CUDA_OK(cudaStreamSynchronize(s));
   if (residual_history)
     for (int k = 0; k <= iters; ++k) residual_history[k] = std::sqrt(std::max(host.rho[k], 0.0));
@@ -947,9 +1123,13 @@ tsn_status read_cg_state(const tsn_plan* P, int iters, double* residual_history,
     status->completed_iterations = host.completed;
     status->positive_curvature = host.curvature_ok;
     status->finite = host.finite_ok && std::isfinite(host.rho[iters]);
-    status->timeout = 0;
+    status->timeout = tc_err != 0;
     status->residual0 = std::sqrt(std::max(host.rho[0], 0.0));
     status->residual_final = std::sqrt(std::max(host.rho[iters], 0.0));
+  }
+  if (tc_err) {
+    set_last_error("a tensor-core interpolation launch gave up a bounded wait");
+    return TSN_ERR_TIMEOUT;
   }
   if (!host.finite_ok || !std::isfinite(host.rho[iters])) return TSN_ERR_NONFINITE;
   if (!host.curvature_ok) return TSN_ERR_CURVATURE;
@@ -1230,14 +1410,14 @@ tsn_status tsn_profile_stages(tsn_plan* plan, const void* y, const void* smaps, 
           o.panel = plan->spanel.as<__half>();
           o.rows = plan->M;
           o.coils = plan->C;
-          launch_interp(plan->view[TSN_VIEW_G].v, plan->panel.as<__half>(), plan->rowh, true, EPI_PANEL, false, o, s);
+          run_interp(plan, TSN_VIEW_G, 1, EPI_PANEL, o, s);
         } break;
         case TSN_STAGE_INTERP_ADJ: {
           InterpOut o;
           o.c64 = plan->grid.as<float2>();
           o.rows = grid_cells(plan);
           o.coils = plan->C;
-          launch_interp(plan->view[TSN_VIEW_GT].v, plan->spanel.as<__half>(), plan->rowh, true, EPI_GRID, true, o, s);
+          run_interp(plan, TSN_VIEW_GT, 1, EPI_GRID, o, s);
         } break;
         case TSN_STAGE_INV_COLS: launch_inv_cols(f, plan->grid.as<float2>(), z_cols, s); break;
         case TSN_STAGE_INV_ROWS:

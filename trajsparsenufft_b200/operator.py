@@ -43,10 +43,14 @@ def _dev_ptr(t, dtype, shape, name):
     return C.c_void_p(t.data_ptr())
 
 
+INTERP = {"auto": 0, "mma_sp": 1, "tcgen05": 2}
+
+
 def plan_desc(im_size=256, grid_size=512, coils=8, width=6, planner="optimized", policy="morton",
-              seed=20260823, threads=0, reference_layout=False, device=None, dims=2) -> PlanDesc:
+              seed=20260823, threads=0, reference_layout=False, device=None, dims=2, interp="auto") -> PlanDesc:
     d = PlanDesc()
     check(lib().tsn_plan_desc_default(C.byref(d)))
+    d.interp = INTERP[interp]
     d.im_size, d.grid_size, d.coils, d.kernel_width = im_size, grid_size, coils, width
     d.dims = int(dims)
     d.planner, d.policy, d.seed, d.threads = _lib.PLANNER[planner], _lib.POLICY[policy], seed, threads
@@ -82,15 +86,28 @@ class Plan:
             "nnz": list(info.nnz), "pack_bytes": list(info.pack_bytes), "workspace_bytes": info.workspace_bytes,
             "plan_seconds": info.plan_seconds, "interp": info.interp, "dims": self.dims,
         }
+        self.interp = {v: k for k, v in INTERP.items()}.get(info.interp, str(info.interp))
+
+    def device_error(self) -> int:
+        """Nonzero once a tensor-core interpolation launch of this plan gave up a bounded wait
+        (read at call time: synchronize the plan's streams first)."""
+        info = PlanInfo()
+        check(lib().tsn_plan_get_info(self._h, C.byref(info)))
+        return int(info.device_error)
 
     # ---- construction ------------------------------------------------------------------
     @classmethod
     def from_trajectory(cls, trajectory, *, im_size=256, grid_size=512, coils=8, width=6, planner="optimized",
-                        policy="morton", seed=20260823, threads=0, reference_layout=False, device=None) -> "Plan":
+                        policy="morton", seed=20260823, threads=0, reference_layout=False, device=None,
+                        interp="auto") -> "Plan":
+        """Pack a trajectory once (C++ planner) and upload both views.  interp chooses the sparse
+        interpolation kernel: "mma_sp" (warp mma.sp per 16-row tile), "tcgen05" (tcgen05.mma.sp
+        with TMA-gathered operands; real-coefficient pack with 8 coils) or "auto"."""
         traj = np.asarray(trajectory, dtype=np.float32)
         dims = 3 if traj.ndim == 2 and traj.shape[1] == 3 else 2
         t = np.ascontiguousarray(traj.reshape(-1, dims))
-        d = plan_desc(im_size, grid_size, coils, width, planner, policy, seed, threads, reference_layout, device, dims)
+        d = plan_desc(im_size, grid_size, coils, width, planner, policy, seed, threads, reference_layout, device, dims,
+                      interp)
         h = C.c_void_p()
         check(lib().tsn_plan_create_from_trajectory(ptr(t, C.c_float), t.shape[0], C.byref(d), C.byref(h)))
         return cls(h)
