@@ -12,7 +12,9 @@ available); the measurement is the operator applied to the phantom plus 1e-3 rms
                     [--config headline|cfg0|batch48|grad4]
 
 --config batch48 reconstructs a seeded uneven batch of 48 cases per step through the batched
-graph and reports the plain per-case drop-in (one solve after another) beside it.
+graph and reports the plain per-case drop-in (one solve after another) beside it.  The default
+(headline) line also carries both comparisons, measured after the headline with 3 steps each
+(--headline-only skips them).
 --config grad4 times differentiable unrolled reconstructions (forward + hand-written backward,
 gradients w.r.t. k-space data, coil maps and x0) of 4 cases per step.
 
@@ -376,7 +378,35 @@ def run_ours(args, cfg) -> dict:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"], out["accuracy"] = cpu_checks(cfg, traj, x_np, s_np, y.cpu().numpy(),
                                                           y_clean.cpu().numpy(), x_out.cpu().numpy(), density)
+    if rank == 0 and world == 1 and not args.headline_only:
+        out.update(side_configs(args))
     return out if rank == 0 else None
+
+
+def side_configs(args) -> dict:
+    """The metric's "batched/grad vs plain" half, measured after the headline in the same run:
+    the 48-case uneven batch (batched graph against the plain per-case drop-in) and the
+    differentiable 4-case unrolled recon (gradients against the forward-only and the plain
+    graph solver), each with 3 warm-up and 3 timed steps of its own configuration."""
+    import copy
+    sub = copy.copy(args)
+    sub.steps, sub.warmup = 3, 3
+    b = run_batch(sub, dict(CONFIGS["batch48"]))
+    g = run_grad(sub, dict(CONFIGS["grad4"]))
+    return {
+        "batched_vs_plain": {
+            "config": b["config"]["workload"], "batched_recons_per_s": b["value"],
+            "plain_per_case_recons_per_s": b["plain_per_case"]["value"], "ratio": b["batch_speedup"],
+            "nonuniform_samples_per_s": b["nonuniform_samples_per_s"], "plan_seconds": b["config"]["plan_seconds"],
+            "steps": sub.steps, "warmup": sub.warmup},
+        "grad_vs_plain": {
+            "config": g["config"]["workload"], "recons_per_s_with_gradients": g["value"],
+            "forward_only_recons_per_s": g["forward_only"]["value"],
+            "plain_graph_solver_recons_per_s": g["plain_graph_solver"]["value"],
+            "backward_over_forward": g["backward_over_forward"],
+            "ratio_with_gradients_over_plain": round(g["value"] / g["plain_graph_solver"]["value"], 4),
+            "steps": sub.steps, "warmup": sub.warmup},
+    }
 
 
 def cpu_checks(cfg, traj, x_np, s_np, y_np, y_clean_gpu, x_gpu, density) -> tuple[dict, dict]:
@@ -1003,6 +1033,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", choices=tuple(CONFIGS), default="headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the batch48 / grad4 comparisons that follow the headline line's measurement")
     ap.add_argument("--interp", choices=("auto", "mma_sp", "tcgen05"), default="auto",
                     help="sparse interpolation kernel of the plans (headline configuration)")
     ap.add_argument("--streams", type=int, default=0, help="batch48: concurrent case streams (default 4)")

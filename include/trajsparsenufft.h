@@ -72,10 +72,17 @@ enum { TSN_VIEW_G = 0, TSN_VIEW_GT = 1 };
 enum { TSN_INTERP_AUTO = 0, TSN_INTERP_MMA_SP = 1, TSN_INTERP_TCGEN05 = 2 };
 /* Plan flags. */
 enum {
-  TSN_FLAG_REFERENCE_LAYOUT = 1 << 0 /* complex real/imag packs, image at [0,N) (reference pack format);
-                                        default for trajectory plans is the real-coefficient pack
-                                        with the image centred on the grid (same operator, half the
-                                        coefficient bytes) */
+  TSN_FLAG_REFERENCE_LAYOUT = 1 << 0, /* complex real/imag packs, image at [0,N) (reference pack format);
+                                         default for trajectory plans is the real-coefficient pack
+                                         with the image centred on the grid (same operator, half the
+                                         coefficient bytes) */
+  TSN_FLAG_REFERENCE_STEPS = 1 << 1   /* also keep an FP32-class operator for the CG's reference
+                                         steps (tsn_cg_options): the same packs with every
+                                         coefficient split into an FP16 high part and an FP16
+                                         residual (the reference's "split2" matrix mode,
+                                         reference_sparse_solver.py:80-110), both against the FP16
+                                         high + residual panels.  2D trajectory plans with the
+                                         centred real-coefficient pack only. */
 };
 
 typedef struct tsn_plan_desc {
@@ -205,6 +212,14 @@ tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y
  * nufft_fp16x2_cg_bench.cu:203-222, without the Tikhonov term), else coil images [C][N][N]. */
 tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x,
                        tsn_stream_t stream);
+/* The FP32-class operators of a plan built with TSN_FLAG_REFERENCE_STEPS (the reference's
+ * forward_reference / adjoint_reference, reference_sparse_solver.py:590-630, which its CG uses
+ * for scheduled reference steps): same arguments and units as tsn_forward / tsn_adjoint, every
+ * KB weight applied as its FP16 high part plus its FP16 residual.  TSN_ERR_ARG on other plans. */
+tsn_status tsn_forward_reference(tsn_plan* plan, const void* x, const void* smaps, void* y,
+                                 tsn_stream_t stream);
+tsn_status tsn_adjoint_reference(tsn_plan* plan, const void* y, const void* smaps, void* x,
+                                 tsn_stream_t stream);
 /* CG-SENSE on (A^H W A + lambda) x = A^H W y from x0 = 0, operator divided by operator_scale
  * (launch_cg, nufft_fp16x2_cg_bench.cu:241-268; reference_sparse_solver.py cg_sense).
  * density (W, [M]) may be NULL.  The whole solve runs as one CUDA graph (captured on first
@@ -222,7 +237,16 @@ tsn_status tsn_cg_sense(tsn_plan* plan, const void* y, const void* smaps, const 
 typedef struct tsn_cg_options {
   int32_t reliable_update_period;
   int32_t reliable_update_direction;
-  int32_t reserved[6];
+  /* Scheduled reference steps (reference_sparse_solver.py:200-332, scheduled_reference_period and
+   * explicit_reference_steps): completed iteration s (1-based) computes A^H W A p through the
+   * FP32-class operator of a plan built with TSN_FLAG_REFERENCE_STEPS when s is a multiple of
+   * scheduled_reference_period (0: none) or bit s-1 of reference_steps is set (s <= 64).  When
+   * any reference step or reliable update is asked for on such a plan, the right-hand side and
+   * the reliable residuals use that operator too, as in the reference. */
+  int32_t scheduled_reference_period;
+  int32_t reserved0;
+  uint64_t reference_steps;
+  int32_t reserved[2];
 } tsn_cg_options;
 tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, const float* density,
                            float lambda, float operator_scale, int32_t iters,

@@ -14,7 +14,8 @@ unnormalized inverse FFT, crop, deapodize, coil combine with conj(S).
 ``KbSenseOperator3`` is the same operator for volumes (real weights, centred image).
 
 ``cg_sense`` restates the CG recursion with its status dictionary
-(reference_sparse_solver.py:200-332, without the reliable-update options).
+(reference_sparse_solver.py:200-332, without the reliable-update options);
+``cg_sense_scheduled`` adds its scheduled reference steps.
 """
 
 from __future__ import annotations
@@ -28,7 +29,7 @@ import scipy.sparse as sp
 from . import kb
 
 PANEL_MODES = ("fp64", "fp32", "fp16", "split2")
-MATRIX_MODES = ("fp64", "fp32", "fp16")
+MATRIX_MODES = ("fp64", "fp32", "fp16", "fp16x2")
 
 
 def _quantize_matrix(values: np.ndarray, mode: str) -> np.ndarray:
@@ -38,6 +39,9 @@ def _quantize_matrix(values: np.ndarray, mode: str) -> np.ndarray:
         return values.astype(np.float32).astype(np.float64)
     if mode == "fp16":
         return values.astype(np.float16).astype(np.float64)
+    if mode == "fp16x2":  # FP16 high part + FP16 residual (the FP32-class reference-step views)
+        hi = values.astype(np.float16).astype(np.float64)
+        return hi + (values - hi).astype(np.float16).astype(np.float64)
     raise ValueError(mode)
 
 
@@ -242,6 +246,45 @@ def cg_sense(forward, adjoint, data, iterations: int, lam: float, operator_scale
         p = r + beta * p
         rs_old = rs_new
         status["completed_iterations"] = iteration + 1
+    return x, residuals, status
+
+
+def cg_sense_scheduled(forward, adjoint, ref_forward, ref_adjoint, data, iterations: int, lam: float,
+                       scheduled_reference_period: int = 0, explicit_reference_steps=()):
+    """CG with scheduled reference steps (reference_sparse_solver.py:200-332, without reliable
+    updates): completed iteration s applies the normal operator through ref_forward /
+    ref_adjoint when s is a multiple of scheduled_reference_period or listed in
+    explicit_reference_steps; the right-hand side comes from ref_adjoint (rhs_adjoint of the
+    reference when a reference step is planned).  Returns (x, residual history, status)."""
+    steps = frozenset(int(v) for v in explicit_reference_steps)
+    status = {"finite": True, "positive_curvature": True, "completed_iterations": 0, "failure": None,
+              "scheduled_reference_steps": []}
+    b = ref_adjoint(np.asarray(data))
+    x = np.zeros_like(b)
+    r = b.copy()
+    p = r.copy()
+    rs_old = float(np.vdot(r, r).real)
+    residuals = [math.sqrt(max(rs_old, 0.0))]
+    for iteration in range(iterations):
+        done = iteration + 1
+        use_ref = done in steps or (scheduled_reference_period > 0 and done % scheduled_reference_period == 0)
+        if use_ref:
+            ap = ref_adjoint(ref_forward(p)) + lam * p
+            status["scheduled_reference_steps"].append(done)
+        else:
+            ap = adjoint(forward(p)) + lam * p
+        denom = float(np.vdot(p, ap).real)
+        if not math.isfinite(denom) or denom <= 0.0:
+            status.update(positive_curvature=False, failure=f"nonpositive_curvature_iteration_{iteration}")
+            break
+        alpha = rs_old / max(denom, 1e-30)
+        x = x + alpha * p
+        r = r - alpha * ap
+        rs_new = float(np.vdot(r, r).real)
+        residuals.append(math.sqrt(max(rs_new, 0.0)))
+        p = r + (rs_new / max(rs_old, 1e-30)) * p
+        rs_old = rs_new
+        status["completed_iterations"] = done
     return x, residuals, status
 
 

@@ -83,3 +83,28 @@ def test_expanded_rho_does_not_drift_on_long_solves():
     x, hist, rel = _fused_cg(normal, b, 60, n)
     assert hist[-1] < 1e-8 * hist[0]
     assert max(rel) < 1e-3
+
+
+def test_scheduled_reference_steps_oracle():
+    """oracle cg_sense_scheduled (reference_sparse_solver.py:249-260): completed iterations that
+    are multiples of the period or listed explicitly take the reference operator; with the same
+    operator on both sides it is the plain CG, and with every step on the reference operator it
+    is the plain CG of that operator (its right-hand side included)."""
+    rng = np.random.default_rng(3)
+    n = 24
+    a = rng.standard_normal((40, n)) + 1j * rng.standard_normal((40, n))
+    a_low = (a + 1e-3 * rng.standard_normal(a.shape)).astype(np.complex128)
+    data = rng.standard_normal(40) + 1j * rng.standard_normal(40)
+    fwd, adj = (lambda v: a_low @ v), (lambda v: a_low.conj().T @ v)
+    rfwd, radj = (lambda v: a @ v), (lambda v: a.conj().T @ v)
+    x0, h0, s0 = oop.cg_sense(fwd, adj, data, 8, 1e-3)
+    x1, h1, s1 = oop.cg_sense_scheduled(fwd, adj, fwd, adj, data, 8, 1e-3, scheduled_reference_period=2)
+    np.testing.assert_allclose(x1, x0, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(h1, h0, rtol=1e-12)
+    assert s1["scheduled_reference_steps"] == [2, 4, 6, 8]
+    xr, hr, _ = oop.cg_sense(rfwd, radj, data, 8, 1e-3)
+    x2, h2, _ = oop.cg_sense_scheduled(fwd, adj, rfwd, radj, data, 8, 1e-3, scheduled_reference_period=1)
+    np.testing.assert_allclose(x2, xr, rtol=1e-12, atol=1e-12)
+    _, _, s3 = oop.cg_sense_scheduled(fwd, adj, rfwd, radj, data, 8, 1e-3, scheduled_reference_period=3,
+                                      explicit_reference_steps=(5, 7))
+    assert s3["scheduled_reference_steps"] == [3, 5, 6, 7]

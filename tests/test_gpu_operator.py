@@ -306,3 +306,79 @@ def test_reliable_update_cg_matches_fp64(direction):
     # the replaced residuals (after iterations 10 and 20) follow the FP64 reliable residuals
     np.testing.assert_allclose(hist[[period, 2 * period]], res_ref[[period, 2 * period]], rtol=2e-2)
     np.testing.assert_allclose(hist[:period], res_ref[:period], rtol=2e-3)
+
+
+def test_reference_operator_is_fp32_class():
+    """tsn_forward_reference / tsn_adjoint_reference (the reference's forward_reference /
+    adjoint_reference): every KB weight as FP16 high part + FP16 residual, FP16x2 panels, FP32
+    FFTs.  Gates: within 1e-6 rel of the FP64 KB operator (its emulation is 5e-8 away; the
+    FP16-weight operator is 7e-5 away) and of the oracle's emulation of the same split; the plain
+    operators of the same plan stay the FP16-weight ones; plans without the views refuse."""
+    from trajsparsenufft_b200._lib import TsnError
+    from trajsparsenufft_b200.operator import Plan
+    traj, x, s, n, g, c, j, readout = case("cfg0")
+    plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=j, reference_steps=True)
+    xt, st, _ = torch_inputs("cfg0")
+    rng = np.random.default_rng(11)
+    yr = (rng.standard_normal((c, len(traj))) + 1j * rng.standard_normal((c, len(traj)))).astype(np.complex64)
+    yt = torch.from_numpy(yr).cuda()
+    f64 = oop.KbSenseOperator(traj, n, g, j, workers=8)
+    ref = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16x2", panel_mode="split2", workers=8)
+    emu = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16", panel_mode="split2", workers=8)
+    y_ref, a_ref = plan.forward(xt, st, reference=True), plan.adjoint(yt, st, reference=True)
+    y_pl, a_pl = plan.forward(xt, st), plan.adjoint(yt, st)
+    torch.cuda.synchronize()
+    y64, a64 = f64.forward(x, s), f64.adjoint(yr, s)
+    errs = {"fwd_ref_vs_f64": rel_l2(y_ref.cpu().numpy(), y64), "adj_ref_vs_f64": rel_l2(a_ref.cpu().numpy(), a64),
+            "fwd_ref_vs_emu": rel_l2(y_ref.cpu().numpy(), ref.forward(x, s)),
+            "adj_ref_vs_emu": rel_l2(a_ref.cpu().numpy(), ref.adjoint(yr, s)),
+            "fwd_plain_vs_f64": rel_l2(y_pl.cpu().numpy(), y64), "adj_plain_vs_f64": rel_l2(a_pl.cpu().numpy(), a64)}
+    print(errs)
+    assert max(errs["fwd_ref_vs_f64"], errs["adj_ref_vs_f64"], errs["fwd_ref_vs_emu"], errs["adj_ref_vs_emu"]) <= 1e-6, errs
+    assert rel_l2(y_pl.cpu().numpy(), emu.forward(x, s)) <= 2e-5
+    assert rel_l2(a_pl.cpu().numpy(), emu.adjoint(yr, s)) <= 2e-5
+    with pytest.raises(TsnError, match="TSN_FLAG_REFERENCE_STEPS"):
+        _plan("cfg0").forward(xt, st, reference=True)
+
+
+def test_reference_steps_follow_the_reference_schedule():
+    """Scheduled reference steps (reference_sparse_solver.py cg_sense: scheduled_reference_period,
+    explicit_reference_steps): on a plan built with reference_steps=True, the chosen iterations
+    apply the normal operator through the FP32-class views, and so does the right-hand side.
+    Gates: a mixed schedule (every 3rd iteration and iteration 5) and an all-reference schedule
+    match the oracle's restatement of the schedule (FP64 CG over the emulated operators) within
+    1e-4 rel, with residual histories within 2e-3 (2e-2 for the last two, small residuals of the
+    undersampled case) -- the FP32 vectors of the device CG, not the operators, set that floor;
+    asking for reference steps on a plan without them is an argument error."""
+    from trajsparsenufft_b200._lib import TsnError
+    from trajsparsenufft_b200.operator import Plan
+    traj, x, s, n, g, c, j, readout = case("cfg0")
+    plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=j, reference_steps=True)
+    _, st, yt = torch_inputs("cfg0")
+    y = measurement("cfg0")
+    f64 = oop.KbSenseOperator(traj, n, g, j, workers=8)
+    emu = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16", panel_mode="split2", workers=8)
+    ref = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16x2", panel_mode="split2", workers=8)
+    x64, _, _ = oop.cg_sense(lambda v: f64.forward(v, s), lambda v: f64.adjoint(v, s), y, 10, 1e-4)
+    report = {}
+    for period, steps in ((1, ()), (3, (5,)), (0, (2, 7))):
+        xg, hg, sg = plan.cg_sense(yt, st, lam=1e-4, iters=10, scheduled_reference_period=period,
+                                   reference_steps=steps)
+        assert sg["positive_curvature"] and sg["finite"] and sg["completed_iterations"] == 10
+        xo, ho, so = oop.cg_sense_scheduled(
+            lambda v: emu.forward(v, s), lambda v: emu.adjoint(v, s), lambda v: ref.forward(v, s),
+            lambda v: ref.adjoint(v, s), y, 10, 1e-4, scheduled_reference_period=period,
+            explicit_reference_steps=steps)
+        e = rel_l2(xg.cpu().numpy(), xo)
+        eh = np.abs(np.asarray(hg) / np.asarray(ho) - 1)
+        report[(period, steps)] = (so["scheduled_reference_steps"], e, rel_l2(xg.cpu().numpy(), x64), eh.max())
+        assert e <= 1e-4, report
+        assert eh[:-2].max() <= 2e-3 and eh.max() <= 2e-2, report
+    print(report)
+    assert report[(3, (5,))][0] == [3, 5, 6, 9] and report[(0, (2, 7))][0] == [2, 7]
+    x_plain, _, _ = plan.cg_sense(yt, st, lam=1e-4, iters=10)
+    x_again, _, _ = _plan("cfg0").cg_sense(yt, st, lam=1e-4, iters=10)
+    # the plain solve of a plan with reference views is the plain solve
+    np.testing.assert_array_equal(x_plain.cpu().numpy(), x_again.cpu().numpy())
+    with pytest.raises(TsnError, match="TSN_FLAG_REFERENCE_STEPS"):
+        _plan("cfg0").cg_sense(yt, st, lam=1e-4, iters=10, scheduled_reference_period=2)

@@ -22,6 +22,7 @@ POLICY = {"trajectory": 0, "morton": 1, "overlap": 2, "packing256": 3}
 ILLEGAL = {"split24": 0, "csr_residual": 1}
 VIEW = {"G": 0, "G_T": 1}
 FLAG_REFERENCE_LAYOUT = 1
+FLAG_REFERENCE_STEPS = 2
 STAGES = ("fwd_rows", "fwd_cols", "interp_fwd", "interp_adj", "inv_cols", "inv_rows", "cg_update", "fwd_mid",
           "inv_mid")
 
@@ -29,7 +30,7 @@ EXPORTED = (
     "tsn_version", "tsn_get_last_error_string", "tsn_plan_desc_default", "tsn_kb_interpolation_csr",
     "tsn_kb_deapodization", "tsn_kb_weights_csr3", "tsn_kb_deapodization3", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
     "tsn_plan_create_from_pack", "tsn_plan_create_from_trajectory", "tsn_plan_destroy", "tsn_plan_get_info",
-    "tsn_forward", "tsn_adjoint", "tsn_cg_sense", "tsn_cg_sense_ex", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
+    "tsn_forward", "tsn_adjoint", "tsn_forward_reference", "tsn_adjoint_reference", "tsn_cg_sense", "tsn_cg_sense_ex", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
     "tsn_fft_forward_panel", "tsn_fft_adjoint_image", "tsn_profile_stages", "tsn_fft_adjoint_image_static",
     "tsn_interp_component",
 )
@@ -64,7 +65,8 @@ class PlanInfo(C.Structure):
 
 class CgOptions(C.Structure):
     _fields_ = [("reliable_update_period", C.c_int32), ("reliable_update_direction", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("scheduled_reference_period", C.c_int32), ("reserved0", C.c_int32),
+                ("reference_steps", C.c_uint64), ("reserved", C.c_int32 * 2)]
 
 
 class CgStatus(C.Structure):
@@ -110,6 +112,8 @@ def lib() -> C.CDLL:
         "tsn_plan_get_info": (C.c_int, [P, C.POINTER(PlanInfo)]),
         "tsn_forward": (C.c_int, [P, P, P, P, P]),
         "tsn_adjoint": (C.c_int, [P, P, P, P, P]),
+        "tsn_forward_reference": (C.c_int, [P, P, P, P, P]),
+        "tsn_adjoint_reference": (C.c_int, [P, P, P, P, P]),
         "tsn_cg_sense": (C.c_int, [P, P, P, P, F32, F32, I32, P, PF64, C.POINTER(CgStatus), P]),
         "tsn_cg_sense_ex": (C.c_int, [P, P, P, P, F32, F32, I32, C.POINTER(CgOptions), P, PF64,
                                       C.POINTER(CgStatus), P]),

@@ -5,6 +5,7 @@
 #include <sys/mman.h>
 
 #include <cstdint>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -73,6 +74,15 @@ inline uint16_t f64_to_f16_bits(double v) {
 }
 
 inline bool f16_bits_nonzero(uint16_t h) { return (h & 0x7FFFu) != 0; }
+
+// Exact binary16 -> binary64 (sign, 5-bit exponent, 10-bit fraction; subnormals, inf, NaN).
+inline double f16_bits_to_f64(uint16_t h) {
+  const int e = (h >> 10) & 0x1F, m = h & 0x3FF;
+  const double sign = (h & 0x8000u) ? -1.0 : 1.0;
+  if (e == 0) return sign * std::ldexp(static_cast<double>(m), -24);
+  if (e == 31) return m ? std::nan("") : sign * HUGE_VAL;
+  return sign * std::ldexp(static_cast<double>(1024 + m), e - 25);
+}
 
 // CPython random.Random: MT19937 seeded by init_by_array over the 32-bit words of
 // abs(seed) (a zero seed is the single word 0), random() = 53-bit double from two

@@ -90,7 +90,7 @@ constexpr int kGatherAhead = 1;
 // Writes one finished item: split chunks publish their accumulators and the last chunk of
 // the group reduces all chunks in chunk order; whole groups and finishing chunks apply the
 // epilogue.
-template <int ROWH, int NCOMP, int NA, int EPI, bool CONJ>
+template <int ROWH, int NCOMP, int NA, int EPI, bool CONJ, bool SUMC>
 __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], const InterpView& v,
                                                    const InterpOut& o, const RecordInfo& info, int lane,
                                                    const int32_t (&rows)[2], const float (&wrow)[2], float scale) {
@@ -150,7 +150,10 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
       for (int a2 = 0; a2 < NA; ++a2) {
         const int coil = 4 * a2 + t;
         float re = acc[0][a2][2 * hr], im = acc[0][a2][2 * hr + 1];
-        if constexpr (NCOMP == 2) {
+        if constexpr (NCOMP == 2 && SUMC) {  // real coefficients split into FP16 high + low parts
+          re += acc[1][a2][2 * hr];
+          im += acc[1][a2][2 * hr + 1];
+        } else if constexpr (NCOMP == 2) {
           const float qre = acc[1][a2][2 * hr], qim = acc[1][a2][2 * hr + 1];
           if (CONJ) {
             re = re + qim;
@@ -178,7 +181,7 @@ __device__ __forceinline__ void interp_finish_item(float (&acc)[NCOMP][NA][4], c
   }
 }
 
-template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, int STAGES>
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, int STAGES, bool SUMC = false>
 __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpView v, const __half* __restrict__ panel,
                                                                          InterpOut o) {
   constexpr int kStages = STAGES;
@@ -289,7 +292,7 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
     }
     __syncwarp();  // this stage is refilled by the next iteration's record copy
     if (info.flags & kRecLast) {  // last tile of its item
-      interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ>(acc, v, o, info, lane, rows, wrow, scale);
+      interp_finish_item<ROWH, NCOMP, NA, EPI, CONJ, SUMC>(acc, v, o, info, lane, rows, wrow, scale);
 #pragma unroll
       for (int c = 0; c < NCOMP; ++c)
 #pragma unroll
@@ -321,23 +324,29 @@ __global__ void __launch_bounds__(kInterpWarps * 32) interp_mmasp_kernel(InterpV
   cp_async_wait<0>();
 }
 
-template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, int STAGES>
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, int STAGES, bool SUMC = false>
 static void launch_interp_s(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
   const int blocks = (v.n_warps + kInterpWarps - 1) / kInterpWarps;
   const size_t smem = static_cast<size_t>(kInterpWarps) * STAGES * (record_bytes(NCOMP) + 32 * ROWH * 2);
-  auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ, STAGES>;
+  auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ, STAGES, SUMC>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (blocks > 0) k<<<blocks, kInterpWarps * 32, smem, s>>>(v, panel, o);
 }
 
-template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ>
+template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, bool SUMC = false>
 static void launch_interp_t(const InterpView& v, const __half* panel, const InterpOut& o, cudaStream_t s) {
-  if (v.stages == 4) launch_interp_s<ROWH, SPLIT, NCOMP, EPI, CONJ, 4>(v, panel, o, s);
-  else launch_interp_s<ROWH, SPLIT, NCOMP, EPI, CONJ, 3>(v, panel, o, s);
+  if (v.stages == 4) launch_interp_s<ROWH, SPLIT, NCOMP, EPI, CONJ, 4, SUMC>(v, panel, o, s);
+  else launch_interp_s<ROWH, SPLIT, NCOMP, EPI, CONJ, 3, SUMC>(v, panel, o, s);
 }
 
 template <int ROWH>
 static void dispatch_epi(const InterpView& v, const __half* panel, int epi, bool conj, const InterpOut& o, cudaStream_t s) {
+  if (v.sum_components) {  // FP16 high + low coefficient parts of a real pack
+    if (epi == EPI_PANEL) launch_interp_t<ROWH, true, 2, EPI_PANEL, false, true>(v, panel, o, s);
+    else if (epi == EPI_GRID) launch_interp_t<ROWH, true, 2, EPI_GRID, false, true>(v, panel, o, s);
+    else launch_interp_t<ROWH, true, 2, EPI_SAMPLES, false, true>(v, panel, o, s);
+    return;
+  }
   if (v.ncomp == 2) {
     if (epi == EPI_SAMPLES) conj ? launch_interp_t<ROWH, true, 2, EPI_SAMPLES, true>(v, panel, o, s)
                                  : launch_interp_t<ROWH, true, 2, EPI_SAMPLES, false>(v, panel, o, s);

@@ -93,10 +93,13 @@ struct GraphKey {
   int iters;
   uint32_t lam_bits, scale_bits;
   cudaStream_t stream;
-  int reliable;  // reliable-update period * 2 + direction
+  int reliable;       // reliable-update period * 2 + direction
+  int ref_period;     // scheduled reference-step period
+  uint64_t ref_steps; // explicit reference steps
   bool operator<(const GraphKey& o) const {
-    return std::tie(y, smaps, density, x, iters, lam_bits, scale_bits, stream, reliable) <
-           std::tie(o.y, o.smaps, o.density, o.x, o.iters, o.lam_bits, o.scale_bits, o.stream, o.reliable);
+    return std::tie(y, smaps, density, x, iters, lam_bits, scale_bits, stream, reliable, ref_period, ref_steps) <
+           std::tie(o.y, o.smaps, o.density, o.x, o.iters, o.lam_bits, o.scale_bits, o.stream, o.reliable, o.ref_period,
+                    o.ref_steps);
   }
 };
 
@@ -110,6 +113,7 @@ struct tsn_plan {
   tsn_plan_desc desc{};
   int N = 0, G = 0, C = 0, J = 0, ncomp = 0, shift = 0, rowh = 0;
   bool use_tc = false;    // interpolation on tcgen05.mma.sp (TSN_INTERP_TCGEN05)
+  DevView view_ref[2];    // FP32-class views (TSN_FLAG_REFERENCE_STEPS): coefficient high + low parts
   DeviceBuffer tc_error;  // int32, set by a tensor-core launch whose bounded wait gave up
   int dims = 2;  // 2: [N][N] images on a G^2 grid; 3: [N][N][N] volumes on a G^3 grid
   int64_t M = 0;
@@ -352,8 +356,11 @@ void build_tc_steps(tsn_plan* P, DevView& d, const HostView& h, bool rows_are_ce
   d.use_tc = true;
 }
 
-void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells) {
-  DevView& d = P->view[which];
+// Uploads one view into P->view[which], or into `target` (the reference-step views, which
+// leave the plan's info and the tensor-core stream alone).
+void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells, bool cols_are_cells,
+                 DevView* target = nullptr) {
+  DevView& d = target ? *target : P->view[which];
   const int64_t tiles = h.tiles(), groups = h.groups();
   const int ncomp = static_cast<int>(h.a.size());
   const int rec = record_bytes(ncomp);
@@ -458,7 +465,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   }
   if (pos != tiles) fail(TSN_ERR_FORMAT, "group offsets do not cover the tiles");
   const std::vector<int2> ranges = cut_ranges(d.item_ends, tiles, interp_resident_warps(4 * P->C, ncomp, stages));
-  if (P->use_tc) build_tc_steps(P, d, h, rows_are_cells, cols_are_cells);
+  if (P->use_tc && !target) build_tc_steps(P, d, h, rows_are_cells, cols_are_cells);
   d.records.upload(records);
   d.counters.upload(std::vector<int32_t>(std::max(nsplit, 1), 0));
   d.partials.alloc(sizeof(float) * static_cast<size_t>(std::max(slots, 1)) * kPartialFloats * 32);
@@ -480,6 +487,7 @@ void upload_view(tsn_plan* P, int which, const HostView& h, bool rows_are_cells,
   d.n_cols = h.n_cols;
   d.present = true;
   d.share = 0;
+  if (target) return;
   P->info.groups[which] = groups;
   P->info.tiles[which] = tiles;
   P->info.active_rows[which] = h.active_rows;
@@ -776,6 +784,8 @@ tsn_status tsn_plan_create_from_pack(const char* fwd_real, const char* fwd_imag,
     if (!out) fail(TSN_ERR_ARG, "plan output pointer is NULL");
     *out = nullptr;
     check_desc(desc);
+    if (desc->flags & TSN_FLAG_REFERENCE_STEPS)
+      fail(TSN_ERR_UNSUPPORTED, "reference steps are built for trajectory plans (centred real-coefficient pack)");
     if (desc->dims == 3) fail(TSN_ERR_UNSUPPORTED, "pack directories hold image (2D) views");
     if (!fwd_real && !adj_real) fail(TSN_ERR_ARG, "at least one view directory is required");
     const auto t0 = std::chrono::steady_clock::now();
@@ -847,6 +857,9 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
     P->M = m;
     P->dims = desc->dims == 3 ? 3 : 2;
     const bool reference_layout = (desc->flags & TSN_FLAG_REFERENCE_LAYOUT) != 0;
+    const bool reference_steps = (desc->flags & TSN_FLAG_REFERENCE_STEPS) != 0;
+    if (reference_steps && (reference_layout || P->dims == 3))
+      fail(TSN_ERR_UNSUPPORTED, "reference steps are built for 2D plans with the centred real-coefficient pack");
     P->shift = reference_layout ? 0 : P->N / 2;
     for (int64_t i = 0; i < P->dims * m; ++i)
       if (!std::isfinite(traj[i]) || std::fabs(traj[i]) > 0.500001f)
@@ -907,7 +920,7 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
     for (size_t i = 0; i < weights.size(); ++i) weights[i] = std::hypot(kb.re[i], kb.im[i]);
     const SparseView st_g = sample_view(kb.row_ptr, kb.cols, ones, traj, m, P->G);
     const SparseView st_gt = transpose_view(st_g, P->G);
-    HostView hv[2];
+    HostView hv[2], hv_ref[2];
     if (reference_layout) {
       const SparseView re_g = sample_view(kb.row_ptr, kb.cols, kb.re, traj, m, P->G);
       const SparseView im_g = sample_view(kb.row_ptr, kb.cols, kb.im, traj, m, P->G);
@@ -915,6 +928,22 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
       hv[0] = host_view_from_tiles(st_g, {&re_g, &im_g}, desc);
       hv[1] = host_view_from_tiles(st_gt, {&re_gt, &im_gt}, desc);
       P->ncomp = 2;
+    } else if (reference_steps) {
+      // centred real pack plus its FP32-class twin: every weight as FP16 high part + FP16
+      // residual on the same tiles (one planner pass serves both)
+      const SparseView w_g = sample_view(kb.row_ptr, kb.cols, weights, traj, m, P->G);
+      std::vector<double> lows(weights.size());
+      for (size_t i = 0; i < lows.size(); ++i) lows[i] = weights[i] - f16_bits_to_f64(f64_to_f16_bits(weights[i]));
+      const SparseView l_g = sample_view(kb.row_ptr, kb.cols, lows, traj, m, P->G);
+      const SparseView w_gt = transpose_view(w_g, P->G), l_gt = transpose_view(l_g, P->G);
+      hv_ref[0] = host_view_from_tiles(st_g, {&w_g, &l_g}, desc);
+      hv_ref[1] = host_view_from_tiles(st_gt, {&w_gt, &l_gt}, desc);
+      for (int v = 0; v < 2; ++v) {
+        hv[v] = hv_ref[v];
+        hv[v].a.resize(1);
+        hv[v].meta.resize(1);
+      }
+      P->ncomp = 1;
     } else {
       // centred image: the phase exp(2 pi i q c/G) moves into the FFT shift, coefficients are
       // the real KB weights
@@ -933,6 +962,11 @@ tsn_status tsn_plan_create_from_trajectory(const float* traj, int64_t m, const t
     P->use_tc = choose_tc(desc, P->ncomp, P->C);
     upload_view(P.get(), TSN_VIEW_G, hv[0], false, true);
     upload_view(P.get(), TSN_VIEW_GT, hv[1], true, false);
+    if (reference_steps) {
+      upload_view(P.get(), TSN_VIEW_G, hv_ref[0], false, true, &P->view_ref[TSN_VIEW_G]);
+      upload_view(P.get(), TSN_VIEW_GT, hv_ref[1], true, false, &P->view_ref[TSN_VIEW_GT]);
+      for (DevView& d : P->view_ref) d.v.sum_components = 1;
+    }
     allocate_workspaces(P.get());
     setup_tc(P.get());
     P->info.samples = P->M;
@@ -984,11 +1018,17 @@ void need_views(const tsn_plan* P, bool fwd, bool adj) {
 }
 
 // One interpolation launch of a view: the tensor-core kernel when the plan uses it, else the
-// warp mma.sp kernel (on a 1/share slice of the GPU for batched cases).  The tensor-core
+// warp mma.sp kernel (on a 1/share slice of the GPU for batched cases); `reference` selects the
+// FP32-class views of the CG's reference steps.  The tensor-core
 // kernel always runs its one-CTA-per-SM schedule; batched cases then share SMs as they free.
-void run_interp(const tsn_plan* P, int which, int share, int epi, const InterpOut& o, cudaStream_t s) {
-  const DevView& d = P->view[which];
+void run_interp(const tsn_plan* P, int which, int share, int epi, const InterpOut& o, cudaStream_t s,
+                bool reference = false) {
   const __half* panel = which == TSN_VIEW_G ? P->panel.as<__half>() : P->spanel.as<__half>();
+  if (reference) {  // FP32-class views: warp kernel summing the coefficients' high and low parts
+    launch_interp(P->view_ref[which].v, panel, P->rowh, true, epi, false, o, s);
+    return;
+  }
+  const DevView& d = P->view[which];
   if (d.use_tc) {
     launch_interp_tc(d.tc, panel, epi, o, s);
     return;
@@ -997,7 +1037,7 @@ void run_interp(const tsn_plan* P, int which, int share, int epi, const InterpOu
   launch_interp(v, panel, P->rowh, true, epi, which == TSN_VIEW_GT, o, s);
 }
 
-void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cudaStream_t s) {
+void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cudaStream_t s, bool reference = false) {
   const FftArgs f = fft_args(P, smaps);
   CgState* st = P->state.as<CgState>();
   const int64_t n = image_pixels(P) * (smaps ? 1 : P->C);
@@ -1011,7 +1051,7 @@ void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cud
   o.scale_ptr = &st->sigma_x;
   o.scale_inv = 1;
   o.scale_mul = f.gs();
-  run_interp(P, TSN_VIEW_G, 1, EPI_SAMPLES, o, s);
+  run_interp(P, TSN_VIEW_G, 1, EPI_SAMPLES, o, s, reference);
 }
 
 // Cuts (once per share value, outside any stream capture) the interpolation warp runs for a
@@ -1030,7 +1070,8 @@ void prepare_share(tsn_plan* P, int share) {
   }
 }
 
-void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cudaStream_t s, int share = 1) {
+void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cudaStream_t s, int share = 1,
+                          bool reference = false) {
   CgState* st = P->state.as<CgState>();
   launch_norm_partials(static_cast<const float2*>(y), P->M * P->C, P->norm_parts.as<double>(), s);
   launch_split_samples(static_cast<const float2*>(y), density, P->M, P->C, P->spanel.as<__half>(),
@@ -1039,16 +1080,24 @@ void enqueue_adjoint_grid(tsn_plan* P, const void* y, const float* density, cuda
   o.c64 = P->grid.as<float2>();
   o.rows = grid_cells(P);
   o.coils = P->C;
-  run_interp(P, TSN_VIEW_GT, share, EPI_GRID, o, s);
+  run_interp(P, TSN_VIEW_GT, share, EPI_GRID, o, s, reference);
 }
 
 // The CG-SENSE solve (launch_cg, nufft_fp16x2_cg_bench.cu:241-268). With reliable_period > 0,
 // after every reliable_period-th iteration except the last the recursive residual is replaced
-// by r = b - M x through the same operator and p restarts as r (direction 0) or continues as
-// r + beta p (direction 1), as in reference_sparse_solver.py:297-323.
+// by r = b - M x and p restarts as r (direction 0) or continues as r + beta p (direction 1), as
+// in reference_sparse_solver.py:297-323.  Reference steps (completed iteration s a multiple of
+// ref_period, or bit s-1 of ref_steps) take A^H W A p through the plan's FP32-class views; when
+// the plan has them and any reference step or reliable update is asked for, the right-hand side
+// and the reliable residuals use them too (rhs_adjoint / reliable_forward of :200-332).
 void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* density, float lambda, float scale,
                 int iters, void* x, cudaStream_t s, int share = 1, int reliable_period = 0,
-                int reliable_direction = 0) {
+                int reliable_direction = 0, int ref_period = 0, uint64_t ref_steps = 0) {
+  const bool have_ref = P->view_ref[TSN_VIEW_G].present && P->view_ref[TSN_VIEW_GT].present;
+  const bool ref_needed = have_ref && (reliable_period > 0 || ref_period > 0 || ref_steps != 0);
+  auto ref_step = [&](int k) {  // iteration k (0-based) completes iteration k + 1
+    return have_ref && ((k < 64 && ((ref_steps >> k) & 1ull)) || (ref_period > 0 && (k + 1) % ref_period == 0));
+  };
   const FftArgs f = fft_args(P, smaps, share);
   CgState* st = P->state.as<CgState>();
   const float inv_s2 = 1.0f / (scale * scale);
@@ -1057,7 +1106,7 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
   float2 *R = P->r.as<float2>(), *Pv = P->p.as<float2>(), *AP = P->ap.as<float2>();
   double *pap = P->parts_pap.as<double>(), *rr = P->parts_rr.as<double>();
   const int lines = f.lines();
-  enqueue_adjoint_grid(P, y, density, s, share);
+  enqueue_adjoint_grid(P, y, density, s, share, ref_needed);
   inv_to_lines(P, f, P->grid.as<float2>(), s);
   launch_inv_rows(f, P->z1.as<float2>(), nullptr, 1, X, R, nullptr, rr, st, 0, inv_s2, 0.f, s);
   int n_rr = settle_partials(P, rr, s);
@@ -1079,12 +1128,13 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
     of.density = density;
     of.rows = P->M;
     of.coils = P->C;
-    run_interp(P, TSN_VIEW_G, share, EPI_PANEL, of, s);
+    const bool ref = ref_step(k);
+    run_interp(P, TSN_VIEW_G, share, EPI_PANEL, of, s, ref);
     InterpOut oa;
     oa.c64 = P->grid.as<float2>();
     oa.rows = grid_cells(P);
     oa.coils = P->C;
-    run_interp(P, TSN_VIEW_GT, share, EPI_GRID, oa, s);
+    run_interp(P, TSN_VIEW_GT, share, EPI_GRID, oa, s, ref);
     inv_to_lines(P, f, P->grid.as<float2>(), s);
     const bool reliable = reliable_period > 0 && (k + 1) % reliable_period == 0 && k + 1 < iters;
     fused = k + 1 < iters && !reliable;
@@ -1097,8 +1147,8 @@ void enqueue_cg(tsn_plan* P, const void* y, const void* smaps, const float* dens
       // r = b - (A^H W A + lambda) x: plain forward of x, then the adjoint into residual mode
       launch_norm_partials(X, image_pixels(P), P->norm_parts.as<double>(), s);
       fwd_chain(P, f, X, 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, P->panel.as<__half>(), s);
-      run_interp(P, TSN_VIEW_G, share, EPI_PANEL, of, s);
-      run_interp(P, TSN_VIEW_GT, share, EPI_GRID, oa, s);
+      run_interp(P, TSN_VIEW_G, share, EPI_PANEL, of, s, ref_needed);
+      run_interp(P, TSN_VIEW_GT, share, EPI_GRID, oa, s, ref_needed);
       inv_to_lines(P, f, P->grid.as<float2>(), s);
       launch_inv_rows(f, P->z1.as<float2>(), R, 3, P->rhs.as<float2>(), nullptr, X, rr, st, k, inv_s2, lam, s);
       n_rr = settle_partials(P, rr, s);
@@ -1146,12 +1196,15 @@ double case_cost(const tsn_plan* P) {
 
 extern "C" {
 
-tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream) {
+static tsn_status forward_entry(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream,
+                                bool reference) {
   try {
     if (!plan || !x || !y) fail(TSN_ERR_ARG, "NULL argument");
     need_aligned({x, smaps, y});
     need_views(plan, true, false);
-    enqueue_forward(plan, x, smaps, y, reinterpret_cast<cudaStream_t>(stream));
+    if (reference && !plan->view_ref[TSN_VIEW_G].present)
+      fail(TSN_ERR_ARG, "the reference operator needs a plan built with TSN_FLAG_REFERENCE_STEPS");
+    enqueue_forward(plan, x, smaps, y, reinterpret_cast<cudaStream_t>(stream), reference);
     CUDA_OK(cudaGetLastError());
     return TSN_OK;
   } catch (const std::exception& e) {
@@ -1159,13 +1212,16 @@ tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y
   }
 }
 
-tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream) {
+static tsn_status adjoint_entry(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream,
+                                bool reference) {
   try {
     if (!plan || !x || !y) fail(TSN_ERR_ARG, "NULL argument");
     need_aligned({x, smaps, y});
     need_views(plan, false, true);
+    if (reference && !plan->view_ref[TSN_VIEW_GT].present)
+      fail(TSN_ERR_ARG, "the reference operator needs a plan built with TSN_FLAG_REFERENCE_STEPS");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    enqueue_adjoint_grid(plan, y, nullptr, s);
+    enqueue_adjoint_grid(plan, y, nullptr, s, 1, reference);
     const FftArgs f = fft_args(plan, smaps);
     inv_to_lines(plan, f, plan->grid.as<float2>(), s);
     launch_inv_rows(f, plan->z1.as<float2>(), static_cast<float2*>(x), 0, nullptr, nullptr, nullptr, nullptr,
@@ -1177,13 +1233,34 @@ tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x
   }
 }
 
+tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream) {
+  return forward_entry(plan, x, smaps, y, stream, false);
+}
+
+tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream) {
+  return adjoint_entry(plan, y, smaps, x, stream, false);
+}
+
+tsn_status tsn_forward_reference(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream) {
+  return forward_entry(plan, x, smaps, y, stream, true);
+}
+
+tsn_status tsn_adjoint_reference(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream) {
+  return adjoint_entry(plan, y, smaps, x, stream, true);
+}
+
 tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, const float* density, float lambda,
                            float operator_scale, int32_t iters, const tsn_cg_options* options, void* x,
                            double* residual_history, tsn_cg_status* status, tsn_stream_t stream) {
   try {
     const int period = options ? options->reliable_update_period : 0;
     const int direction = options ? options->reliable_update_direction : 0;
+    const int ref_period = options ? options->scheduled_reference_period : 0;
+    const uint64_t ref_steps = options ? options->reference_steps : 0;
     if (period < 0 || direction < 0 || direction > 1) fail(TSN_ERR_ARG, "invalid reliable-update options");
+    if (ref_period < 0) fail(TSN_ERR_ARG, "scheduled_reference_period must be >= 0");
+    if ((ref_period > 0 || ref_steps) && plan && !plan->view_ref[TSN_VIEW_G].present)
+      fail(TSN_ERR_ARG, "reference steps need a plan built with TSN_FLAG_REFERENCE_STEPS");
     if (!plan || !y || !smaps || !x) fail(TSN_ERR_ARG, "NULL argument (y, smaps and x are required)");
     if (iters < 0 || iters > kMaxCgIter) fail(TSN_ERR_ARG, "iteration count out of range");
     if (!(operator_scale > 0.0f) || !std::isfinite(lambda)) fail(TSN_ERR_ARG, "invalid operator scale or lambda");
@@ -1191,7 +1268,7 @@ tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, con
     if (reinterpret_cast<uintptr_t>(density) & 3u) fail(TSN_ERR_ARG, "density must be 4-byte aligned");
     need_views(plan, true, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    GraphKey key{y, smaps, density, x, iters, 0, 0, s, period * 2 + direction};
+    GraphKey key{y, smaps, density, x, iters, 0, 0, s, period * 2 + direction, ref_period, ref_steps};
     std::memcpy(&key.lam_bits, &lambda, 4);
     std::memcpy(&key.scale_bits, &operator_scale, 4);
     auto it = plan->graphs.find(key);
@@ -1204,7 +1281,8 @@ tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, con
       }
       cudaGraph_t g = nullptr;
       CUDA_OK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
-      enqueue_cg(plan, y, smaps, density, lambda, operator_scale, iters, x, cap, 1, period, direction);
+      enqueue_cg(plan, y, smaps, density, lambda, operator_scale, iters, x, cap, 1, period, direction, ref_period,
+                 ref_steps);
       const cudaError_t launch_err = cudaGetLastError();
       const cudaError_t end_err = cudaStreamEndCapture(cap, &g);
       if (own) cudaStreamDestroy(cap);
@@ -1223,6 +1301,7 @@ tsn_status tsn_cg_sense_ex(tsn_plan* plan, const void* y, const void* smaps, con
     CUDA_OK(cudaGraphLaunch(it->second, s));
     if (residual_history || status) {
       const tsn_status rc = read_cg_state(plan, iters, residual_history, status, s);
+      if (rc == TSN_ERR_TIMEOUT) fail(TSN_ERR_TIMEOUT, "a bounded device wait gave up during the solve");
       if (rc == TSN_ERR_NONFINITE) fail(TSN_ERR_NONFINITE, "CG produced non-finite values");
       if (rc == TSN_ERR_CURVATURE) fail(TSN_ERR_CURVATURE, "CG denominator <= 0 (positive_curvature = 0)");
     }

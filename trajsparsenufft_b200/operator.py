@@ -99,15 +99,19 @@ class Plan:
     @classmethod
     def from_trajectory(cls, trajectory, *, im_size=256, grid_size=512, coils=8, width=6, planner="optimized",
                         policy="morton", seed=20260823, threads=0, reference_layout=False, device=None,
-                        interp="auto") -> "Plan":
+                        interp="auto", reference_steps=False) -> "Plan":
         """Pack a trajectory once (C++ planner) and upload both views.  interp chooses the sparse
         interpolation kernel: "mma_sp" (warp mma.sp per 16-row tile), "tcgen05" (tcgen05.mma.sp
-        with TMA-gathered operands; real-coefficient pack with 8 coils) or "auto"."""
+        with stacked tiles; real-coefficient pack with 8 coils) or "auto".  reference_steps
+        keeps an FP32-class copy of the operator (coefficients as FP16 high + FP16 residual) for
+        the CG's scheduled reference steps (TSN_FLAG_REFERENCE_STEPS)."""
         traj = np.asarray(trajectory, dtype=np.float32)
         dims = 3 if traj.ndim == 2 and traj.shape[1] == 3 else 2
         t = np.ascontiguousarray(traj.reshape(-1, dims))
         d = plan_desc(im_size, grid_size, coils, width, planner, policy, seed, threads, reference_layout, device, dims,
                       interp)
+        if reference_steps:
+            d.flags |= _lib.FLAG_REFERENCE_STEPS
         h = C.c_void_p()
         check(lib().tsn_plan_create_from_trajectory(ptr(t, C.c_float), t.shape[0], C.byref(d), C.byref(h)))
         return cls(h)
@@ -154,8 +158,10 @@ class Plan:
     def _image_shape(self, smaps):
         return self.image_shape if smaps is not None else self.maps_shape
 
-    def forward(self, x, smaps=None, out=None, stream=None):
-        """y[C, M] = A x (unnormalized NUFFT of x*S_c, or of coil images when smaps is None)."""
+    def forward(self, x, smaps=None, out=None, stream=None, reference=False):
+        """y[C, M] = A x (unnormalized NUFFT of x*S_c, or of coil images when smaps is None).
+        reference=True applies the FP32-class operator of a plan built with
+        reference_steps=True (the reference's forward_reference)."""
         torch = _torch()
         cf = torch.complex64
         xp = _dev_ptr(x, cf, self._image_shape(smaps), "x")
@@ -163,11 +169,13 @@ class Plan:
         if out is None:
             out = torch.empty((self.coils, self.samples), dtype=cf, device=x.device)
         yp = _dev_ptr(out, cf, (self.coils, self.samples), "out")
-        check(lib().tsn_forward(self._h, xp, sp, yp, _stream_handle(stream)))
+        fn = lib().tsn_forward_reference if reference else lib().tsn_forward
+        check(fn(self._h, xp, sp, yp, _stream_handle(stream)))
         return out
 
-    def adjoint(self, y, smaps=None, out=None, stream=None):
-        """x = A^H y: coil-combined image [N, N] with smaps, else coil images [C, N, N]."""
+    def adjoint(self, y, smaps=None, out=None, stream=None, reference=False):
+        """x = A^H y: coil-combined image [N, N] with smaps, else coil images [C, N, N].
+        reference=True: the FP32-class operator (the reference's adjoint_reference)."""
         torch = _torch()
         cf = torch.complex64
         yp = _dev_ptr(y, cf, (self.coils, self.samples), "y")
@@ -175,17 +183,23 @@ class Plan:
         if out is None:
             out = torch.empty(self._image_shape(smaps), dtype=cf, device=y.device)
         xp = _dev_ptr(out, cf, self._image_shape(smaps), "out")
-        check(lib().tsn_adjoint(self._h, yp, sp, xp, _stream_handle(stream)))
+        fn = lib().tsn_adjoint_reference if reference else lib().tsn_adjoint
+        check(fn(self._h, yp, sp, xp, _stream_handle(stream)))
         return out
 
     def cg_sense(self, y, smaps, *, density=None, lam=1e-4, iters=10, operator_scale=1.0, out=None, stream=None,
-                 sync=True, reliable_update_period=0, reliable_update_direction="restart"):
+                 sync=True, reliable_update_period=0, reliable_update_direction="restart",
+                 scheduled_reference_period=0, reference_steps=()):
         """CG-SENSE solve of (A^H W A + lam) x = A^H W y from x0 = 0 (one CUDA graph).
 
         Returns (x, residual history or None, status dict or None).  With sync=False
         the call is fully asynchronous and no host-side status is produced.  A positive
         reliable_update_period replaces the recursive residual by b - M x after every that
-        many iterations, with p restarted ("restart") or continued ("beta").
+        many iterations, with p restarted ("restart") or continued ("beta").  On a plan built
+        with reference_steps=True, completed iterations that are multiples of
+        scheduled_reference_period, or listed in reference_steps (1-based, <= 64), apply the
+        normal operator through the FP32-class coefficients (reference_sparse_solver.py cg_sense,
+        scheduled_reference_period / explicit_reference_steps).
         """
         torch = _torch()
         cf = torch.complex64
@@ -202,6 +216,13 @@ class Plan:
         opts = _lib.CgOptions()
         opts.reliable_update_period = int(reliable_update_period)
         opts.reliable_update_direction = 0 if reliable_update_direction == "restart" else 1
+        opts.scheduled_reference_period = int(scheduled_reference_period)
+        mask = 0
+        for step in reference_steps:
+            if not 1 <= int(step) <= 64:
+                raise ValueError("reference steps are completed iterations 1..64")
+            mask |= 1 << (int(step) - 1)
+        opts.reference_steps = mask
         rc = lib().tsn_cg_sense_ex(self._h, yp, sp, dp, float(lam), float(operator_scale), int(iters),
                                    C.byref(opts), xp, ptr(hist, C.c_double), C.byref(st) if sync else None,
                                    _stream_handle(stream))
