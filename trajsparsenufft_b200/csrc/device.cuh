@@ -27,6 +27,14 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// Programmatic dependent launch. pdl_wait blocks until the kernel this one was launched
+// behind (with cudaLaunchAttributeProgrammaticStreamSerialization) has completed and its
+// writes are visible; pdl_trigger lets the next such kernel of the stream start its prologue.
+// Both return at once in a kernel launched without the attribute.  A kernel reads nothing
+// that an earlier kernel may write, and writes nothing, before pdl_wait.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src));
 }
