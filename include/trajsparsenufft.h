@@ -212,6 +212,19 @@ tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y
  * nufft_fp16x2_cg_bench.cu:203-222, without the Tikhonov term), else coil images [C][N][N]. */
 tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x,
                        tsn_stream_t stream);
+/* Pieces of the CG for callers that run their own (differentiable) recursion: the reference
+ * solver's normal operator `adjoint(forward(p)) + lam p` with its W weighting
+ * (reference_sparse_solver.py:200-332 cg_sense, forward/adjoint of :590-630) and its inner
+ * products.  tsn_normal: q[N][N] = sum_c conj(S_c) F^H W F(S_c p) + lambda p (device arrays;
+ * density W [M] may be NULL), with, when coil_images != NULL, the coil images
+ * F^H W F(S_c p) [C][N][N] before the combine, and, when pq != NULL, Re <p, q> summed in FP64
+ * in a fixed order into the device double *pq.  Same units as tsn_forward / tsn_adjoint.
+ * tsn_rdot: *out (device) = Re <a, b> = sum a.re b.re + a.im b.im over n complex values, FP64,
+ * fixed order.  Both use the plan's workspaces: calls on one plan are ordered by their stream. */
+tsn_status tsn_normal(tsn_plan* plan, const void* p, const void* smaps, const float* density, float lambda,
+                      void* q, void* coil_images, double* pq, tsn_stream_t stream);
+tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, double* out,
+                    tsn_stream_t stream);
 /* The FP32-class operators of a plan built with TSN_FLAG_REFERENCE_STEPS (the reference's
  * forward_reference / adjoint_reference, reference_sparse_solver.py:590-630, which its CG uses
  * for scheduled reference steps): same arguments and units as tsn_forward / tsn_adjoint, every

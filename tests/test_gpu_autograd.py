@@ -172,3 +172,41 @@ def test_graph_captured_gradient_step_matches_eager():
         for leaf, ge in zip(leaves, grads_e):
             rel = float(torch.linalg.vector_norm(leaf.grad - ge) / torch.linalg.vector_norm(ge))
             assert rel <= 1e-6, rel
+
+
+def test_normal_operator_and_fp64_dots_in_cuda():
+    """tsn_normal (q = sum_c conj(S_c) F^H W F(S_c p) + lam p with its coil images and FP64
+    Re <p, q>) and tsn_rdot, which the differentiable CG uses on a GPU plan, against the same
+    operator composed from tsn_forward / tsn_adjoint on coil images with torch (the generic
+    path of autograd._Sense) and against the FP16x2 oracle emulation.  Gates: q and the coil
+    images within 2e-5 rel of both (FP16x2 rounding; the fused path scales its panel by |p|
+    instead of |S p|); the FP64 inner products within 1e-12 rel of numpy's over the same
+    FP32 vectors; a lazily conjugated view is refused."""
+    from trajsparsenufft_b200 import synth
+    from trajsparsenufft_b200.operator import Plan
+    traj, x, s, n, g, c, j, readout = case("grad4")
+    plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=j)
+    w = synth.ramp_density(traj, readout).astype(np.float32)
+    rng = np.random.default_rng(9)
+    p = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    pt, st, wt = torch.from_numpy(p).cuda(), torch.from_numpy(s).cuda(), torch.from_numpy(w).cuda()
+    for _ in range(2):  # repeated calls on one plan: the workspaces carry nothing over
+        q, t, pq = plan.normal(pt, st, density=wt, lam=LAM, coils=True, pq=True)
+        torch.cuda.synchronize()
+    t_ref = plan.adjoint(plan.forward((st * pt).contiguous()) * wt)
+    q_ref = (st.conj() * t_ref).sum(0) + LAM * pt
+    qn, tn = q.cpu().numpy(), t.cpu().numpy()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    assert rel(qn, q_ref.cpu().numpy()) <= 2e-5
+    assert rel(tn, t_ref.cpu().numpy()) <= 2e-5
+    emu = oop.KbSenseOperator(traj, n, g, j, matrix_mode="fp16", panel_mode="split2", workers=8)
+    q_emu = emu.adjoint(emu.forward(p.astype(np.complex128), s) * w, s) + LAM * p
+    assert rel(qn, q_emu) <= 2e-5
+    want = float(np.sum(p.real.astype(np.float64) * qn.real + p.imag.astype(np.float64) * qn.imag))
+    assert abs(float(pq.cpu()) - want) <= 1e-12 * abs(want)
+    q2, _, _ = plan.normal(pt, st, density=wt, lam=LAM)
+    np.testing.assert_array_equal(q2.cpu().numpy(), qn)  # without the extra outputs: the same q
+    d = plan.rdot(pt, q)
+    assert abs(float(d.cpu()) - want) <= 1e-12 * abs(want)
+    with pytest.raises(ValueError):
+        plan.rdot(pt.conj(), q)

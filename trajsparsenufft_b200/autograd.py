@@ -42,6 +42,20 @@ class PlanOps:
     def adjoint_coils(self, y: torch.Tensor) -> torch.Tensor:
         return self.plan.adjoint(y.contiguous())
 
+    def normal(self, p, smaps, density, lam, coils=False, pq=False):
+        """(sum_c conj(S_c) G(S_c p) + lam p, the coil images G(S_c p) or None, Re <p, q> or
+        None) in the plan's kernels (tsn_normal): SENSE expansion, weighting, combine and the
+        FP64 inner product fused into the NUFFT stages."""
+        return self.plan.normal(p.contiguous(), smaps.contiguous(), density=density, lam=lam, coils=coils, pq=pq)
+
+    def rdot(self, a, b):
+        """Re <a, b> in FP64, fixed order (tsn_rdot), as a 0-d device tensor."""
+        return self.plan.rdot(a.contiguous(), b.contiguous())
+
+    def forward_maps(self, x, smaps):
+        """F(S_c x) with the SENSE expansion inside the row transforms (tsn_forward)."""
+        return self.plan.forward(x.contiguous(), smaps.contiguous())
+
 
 def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
     """Re <a, b> = sum(a.re b.re + a.im b.im), accumulated in FP64 (a 0-d tensor), like the graph
@@ -52,10 +66,13 @@ def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
 
 
 class _Sense:
-    """SENSE algebra over a CoilOps object (no autograd inside)."""
+    """SENSE algebra over a CoilOps object (no autograd inside).  When the ops object has
+    `normal` and `rdot` (PlanOps), M p, its coil images and the FP64 inner products run in the
+    plan's CUDA kernels; otherwise they are composed here from forward_coils / adjoint_coils."""
 
     def __init__(self, ops, smaps, density, lam):
         self.ops, self.s, self.w, self.lam = ops, smaps, density, lam
+        self.fused = all(hasattr(ops, k) for k in ("normal", "rdot", "forward_maps"))
 
     def weigh(self, y):
         return y if self.w is None else y * self.w
@@ -66,11 +83,31 @@ class _Sense:
     def combine(self, coils):
         return (self.s.conj() * coils).sum(0)
 
+    def dot(self, a, b):
+        return self.ops.rdot(a, b) if self.fused else _rdot(a, b)
+
+    def A(self, x):
+        """F(S x), the coil k-space of image x."""
+        return self.ops.forward_maps(x, self.s) if self.fused else self.ops.forward_coils(self.s * x)
+
     def M(self, p):
+        if self.fused:
+            return self.ops.normal(p, self.s, self.w, self.lam)[0]
         return self.combine(self.G(self.s * p)) + self.lam * p
+
+    def M_dot(self, p):
+        """(M p, Re <p, M p>)."""
+        if self.fused:
+            q, _, pq = self.ops.normal(p, self.s, self.w, self.lam, pq=True)
+            return q, pq
+        q = self.M(p)
+        return q, _rdot(p, q)
 
     def M_coils(self, p):
         """(M p, the coil images G(S p)) — the second feeds the coil-map gradient."""
+        if self.fused:
+            q, t, _ = self.ops.normal(p, self.s, self.w, self.lam, coils=True)
+            return q, t
         t = self.G(self.s * p)
         return self.combine(t) + self.lam * p, t
 
@@ -132,20 +169,23 @@ class UnrolledCgSense(torch.autograd.Function):
         x = x0.clone()
         r = b.clone() if x0_zero else b - S.M(x0)
         p = r.clone()
-        rho = _rdot(r, r)
+        rho = S.dot(r, r)
         cps = [(x, r, p, rho)]
         need_s = ctx.needs_input_grad[1]
         firsts = []   # q = M p (and the coil images G(S p) when maps need gradients) of each
         for k in range(iters):   # checkpointed step: the backward reuses them instead of recomputing
-            if k % checkpoint == 0:
+            if k % checkpoint == 0 and need_s:
                 q, t = S.M_coils(p)
-                firsts.append((q, t) if need_s else (q,))
+                firsts.append((q, t))
+                gamma = S.dot(p, q)
             else:
-                q = S.M(p)
-            alpha = rho / _rdot(p, q)
+                q, gamma = S.M_dot(p)
+                if k % checkpoint == 0:
+                    firsts.append((q,))
+            alpha = rho / gamma
             x = x + alpha * p
             r = r - alpha * q
-            rho_n = _rdot(r, r)
+            rho_n = S.dot(r, r)
             p = r + (rho_n / rho) * p
             rho = rho_n
             if (k + 1) % checkpoint == 0 and k + 1 < iters:
@@ -187,25 +227,25 @@ class UnrolledCgSense(torch.autograd.Function):
                     q, t = S.M_coils(p)
                 else:
                     q, t = S.M(p), None
-                gamma = _rdot(p, q)
+                gamma = S.dot(p, q)
                 alpha = rho / gamma
                 r_n = r - alpha * q
-                rho_n = _rdot(r_n, r_n)
+                rho_n = S.dot(r_n, r_n)
                 beta = rho_n / rho
                 steps.append((p, q, t, r_n, rho, rho_n, gamma, alpha, beta))
                 p = r_n + beta * p
                 r, rho = r_n, rho_n
             for p, q, t, r_n, rho, rho_n, gamma, alpha, beta in reversed(steps):
                 rb = rb + pb                                   # p' = r' + beta p
-                betab = _rdot(pb, p)
+                betab = S.dot(pb, p)
                 pbk = beta * pb
                 rhob_n = rhob + betab / rho                    # beta = rho' / rho
                 rhobk = -betab * rho_n / (rho * rho)
                 rb = rb + (2.0 * rhob_n) * r_n                 # rho' = |r'|^2
                 qb = -alpha * rb                               # r' = r - alpha q
-                alphab = -_rdot(rb, q)
+                alphab = -S.dot(rb, q)
                 pbk = pbk + alpha * xb                         # x' = x + alpha p
-                alphab = alphab + _rdot(xb, p)
+                alphab = alphab + S.dot(xb, p)
                 rhobk = rhobk + alphab / gamma                 # alpha = rho / gamma
                 gammab = -alphab * rho / (gamma * gamma)
                 pbk = pbk + gammab * q                         # gamma = Re <p, q>
@@ -230,7 +270,7 @@ class UnrolledCgSense(torch.autograd.Function):
             sb = sb + rb.conj() * u                           # b = sum conj(S) F^H W y
             gs = sb
         if need_y:
-            gy = S.weigh(ctx.ops.forward_coils(smaps * rb))
+            gy = S.weigh(S.A(rb))
         return gy, gs, gx0, None, None, None, None, None, None
 
 

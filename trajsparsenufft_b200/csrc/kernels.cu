@@ -1062,7 +1062,7 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
   if (blockIdx.x < lines) issue(blockIdx.x, 2);
   float factor;
   if (mode == 2) factor = f.gs() / st->sigma[iter] * inv_scale2;
-  else if (mode == 3) factor = f.gs() / st->sigma_x * inv_scale2;
+  else if (mode == 3 || mode == 5) factor = f.gs() / st->sigma_x * inv_scale2;
   else factor = inv_scale2 / st->sigma_y;
   const int c = warp;
   const int lane_off = 2 * ((c >> 1) ^ slab_swz(lane, C >> 1)) + (c & 1);
@@ -1099,6 +1099,8 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
         for (int cc = 0; cc < C; ++cc) out[static_cast<size_t>(cc) * pix_n + pix] = cscale(img_s[cc * N + i1], d);
         continue;
       }
+      if (mode == 5 && x)  // the coil images before the combine, [C][N][N]
+        for (int cc = 0; cc < C; ++cc) x[static_cast<size_t>(cc) * pix_n + pix] = cscale(img_s[cc * N + i1], d);
       float2 acc = make_float2(0.f, 0.f);
       for (int cc = 0; cc < C; ++cc) {
         const float2 s = epi_smem ? emaps[cc * N + i1] : f.smaps[static_cast<size_t>(cc) * pix_n + pix];
@@ -1115,10 +1117,10 @@ __global__ void TSN_FFT_BOUNDS(G, (CC <= 8 ? 8 : 16)) inv_rows_kernel(FftArgs f,
         const float2 pv = epi_smem ? eprow[i1] : p[pix];
         acc.x += lambda_scaled * pv.x;
         acc.y += lambda_scaled * pv.y;
-        if (mode == 2) {
+        if (mode == 2 || mode == 5) {
           out[pix] = acc;
           dot += static_cast<double>(pv.x) * acc.x + static_cast<double>(pv.y) * acc.y;
-          if (r) {
+          if (mode == 2 && r) {
             const float2 rv = r[pix];
             dot_r += static_cast<double>(rv.x) * acc.x + static_cast<double>(rv.y) * acc.y;
             dot_a += static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y;
@@ -1427,6 +1429,36 @@ __global__ void reduce_partials_kernel(double* part, int n, int64_t stride) {
 
 void launch_reduce_partials(double* part, int n, cudaStream_t s, int sections, int64_t stride) {
   reduce_partials_kernel<<<sections, 1024, 0, s>>>(part, n, stride);
+}
+
+// FP64 partials of Re <a, b> over n complex values (grid-stride, one per block).
+__global__ void rdot_partials_kernel(const float2* __restrict__ a, const float2* __restrict__ b, int64_t n,
+                                     double* __restrict__ part) {
+  __shared__ double scratch[33];
+  double acc = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 u = a[i], v = b[i];
+    acc += static_cast<double>(u.x) * v.x + static_cast<double>(u.y) * v.y;
+  }
+  const double t = block_sum(acc, scratch);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// out[0] = the sum of n partials, in a fixed order (one block).
+__global__ void sum_partials_to_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
+  __shared__ double red[33];
+  const double t = sum_partials(part, n, red);
+  if (threadIdx.x == 0) out[0] = t;
+}
+
+void launch_rdot(const float2* a, const float2* b, int64_t n, double* parts, double* out, cudaStream_t s) {
+  rdot_partials_kernel<<<kNormParts, 256, 0, s>>>(a, b, n, parts);
+  sum_partials_to_kernel<<<1, 256, 0, s>>>(parts, kNormParts, out);
+}
+
+void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_t s) {
+  sum_partials_to_kernel<<<1, 256, 0, s>>>(parts, n, out);
 }
 
 template <class T>

@@ -198,6 +198,9 @@ void launch_inv_cols(const FftArgs& f, const float2* grid, float2* w1, cudaStrea
 //         Re <r, ap>, <ap, ap> and <r, r> partials at partials + lines, + 2 lines, + 3 lines)
 // mode 3: reliable residual: out = x - (factor*AHAp + lambda p) with x = the right-hand
 //         side b, p = the iterate and factor from the plain forward's sigma_x; rr partials
+// mode 5: normal operator of a plain forward: out = factor*AHAp + lambda p, factor from
+//         sigma_x, <p, out> partials; with x given, also the coil images [C][N][N] of
+//         factor*AHAp before the coil combine
 void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, float2* x, float2* r,
                      const float2* p, double* partials, CgState* st, int iter, float inv_scale2,
                      float lambda_scaled, cudaStream_t s);
@@ -207,6 +210,10 @@ void launch_inv_rows(const FftArgs& f, const float2* w1, float2* out, int mode, 
 void launch_cg_update(int N, int lines, int nparts, float2* x, float2* r, const float2* p, const float2* ap,
                       const double* pap_parts, double* rr_parts, CgState* st, int iter, cudaStream_t s);
 void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters, cudaStream_t s);
+// out[0] = Re <a, b> over n complex values in FP64 (kNormParts partials in parts, fixed order)
+void launch_rdot(const float2* a, const float2* b, int64_t n, double* parts, double* out, cudaStream_t s);
+// out[0] = the sum of n partials in a fixed order
+void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_t s);
 
 void launch_gather_rows_f16(const __half* src, const int32_t* map, int64_t rows, int width, __half* dst,
                             cudaStream_t s);

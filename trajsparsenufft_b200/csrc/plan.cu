@@ -1054,6 +1054,35 @@ void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cud
   run_interp(P, TSN_VIEW_G, 1, EPI_SAMPLES, o, s, reference);
 }
 
+// q = A^H W A p + lambda p through the plan's operator (the CG's normal operator at operator
+// scale 1), with the optional coil images A_c^H W A p before the coil combine and the optional
+// FP64 Re <p, q>: the plain forward's panel scale, both interpolations, the inverse FFTs and
+// the combine epilogue (inv_rows mode 5).
+void enqueue_normal(tsn_plan* P, const void* p, const void* smaps, const float* density, float lambda, void* q,
+                    void* coils, double* pq, cudaStream_t s) {
+  const FftArgs f = fft_args(P, smaps);
+  CgState* st = P->state.as<CgState>();
+  const float2* pv = static_cast<const float2*>(p);
+  launch_norm_partials(pv, image_pixels(P), P->norm_parts.as<double>(), s);
+  fwd_chain(P, f, pv, 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, P->panel.as<__half>(), s);
+  InterpOut of;
+  of.panel = P->spanel.as<__half>();
+  of.density = density;
+  of.rows = P->M;
+  of.coils = P->C;
+  run_interp(P, TSN_VIEW_G, 1, EPI_PANEL, of, s);
+  InterpOut oa;
+  oa.c64 = P->grid.as<float2>();
+  oa.rows = grid_cells(P);
+  oa.coils = P->C;
+  run_interp(P, TSN_VIEW_GT, 1, EPI_GRID, oa, s);
+  inv_to_lines(P, f, P->grid.as<float2>(), s);
+  double* parts = P->parts_rr.as<double>();
+  launch_inv_rows(f, P->z1.as<float2>(), static_cast<float2*>(q), 5, static_cast<float2*>(coils), nullptr, pv, parts, st,
+                  0, 1.0f, lambda, s);
+  if (pq) launch_sum_partials_to(parts, settle_partials(P, parts, s), pq, s);
+}
+
 // Cuts (once per share value, outside any stream capture) the interpolation warp runs for a
 // 1/share slice of the GPU, so cases of a batch run their launches side by side.
 void prepare_share(tsn_plan* P, int share) {
@@ -1239,6 +1268,35 @@ tsn_status tsn_forward(tsn_plan* plan, const void* x, const void* smaps, void* y
 
 tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x, tsn_stream_t stream) {
   return adjoint_entry(plan, y, smaps, x, stream, false);
+}
+
+tsn_status tsn_normal(tsn_plan* plan, const void* p, const void* smaps, const float* density, float lambda, void* q,
+                      void* coil_images, double* pq, tsn_stream_t stream) {
+  try {
+    if (!plan || !p || !smaps || !q) fail(TSN_ERR_ARG, "NULL argument (p, smaps and q are required)");
+    if (!std::isfinite(lambda)) fail(TSN_ERR_ARG, "lambda must be finite");
+    need_aligned({p, smaps, q, coil_images, density});
+    need_views(plan, true, true);
+    enqueue_normal(plan, p, smaps, density, lambda, q, coil_images, pq, reinterpret_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, double* out, tsn_stream_t stream) {
+  try {
+    if (!plan || !a || !b || !out) fail(TSN_ERR_ARG, "NULL argument");
+    if (n < 0) fail(TSN_ERR_ARG, "n must be >= 0");
+    CUDA_OK(cudaSetDevice(plan->desc.device));
+    launch_rdot(static_cast<const float2*>(a), static_cast<const float2*>(b), n, plan->norm_parts.as<double>(), out,
+                reinterpret_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
 }
 
 tsn_status tsn_forward_reference(tsn_plan* plan, const void* x, const void* smaps, void* y, tsn_stream_t stream) {

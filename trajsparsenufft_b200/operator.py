@@ -40,6 +40,8 @@ def _dev_ptr(t, dtype, shape, name):
         raise ValueError(f"{name} must have shape {tuple(shape)}, got {tuple(t.shape)}")
     if not t.is_contiguous():
         raise ValueError(f"{name} must be contiguous")
+    if t.is_complex() and t.is_conj():
+        raise ValueError(f"{name} is a lazily conjugated view: pass {name}.resolve_conj()")
     return C.c_void_p(t.data_ptr())
 
 
@@ -186,6 +188,38 @@ class Plan:
         fn = lib().tsn_adjoint_reference if reference else lib().tsn_adjoint
         check(fn(self._h, yp, sp, xp, _stream_handle(stream)))
         return out
+
+    def normal(self, p, smaps, *, density=None, lam=0.0, out=None, coils=False, pq=False, stream=None):
+        """q = A^H W A p + lam p (tsn_normal): the CG's normal operator on image p [N, N] with
+        coil maps.  coils=True also returns the coil images A_c^H W A p [C, N, N] before the
+        combine; pq=True also returns Re <p, q> as a 0-d FP64 tensor on the device (no sync).
+        Returns (q, coil images or None, Re <p, q> or None)."""
+        torch = _torch()
+        cf = torch.complex64
+        pp = _dev_ptr(p, cf, self.image_shape, "p")
+        sp = _dev_ptr(smaps, cf, self.maps_shape, "smaps")
+        dp = None if density is None else _dev_ptr(density, torch.float32, (self.samples,), "density")
+        if out is None:
+            out = torch.empty(self.image_shape, dtype=cf, device=p.device)
+        qp = _dev_ptr(out, cf, self.image_shape, "out")
+        t = torch.empty(self.maps_shape, dtype=cf, device=p.device) if coils else None
+        tp = None if t is None else _dev_ptr(t, cf, self.maps_shape, "coils")
+        d = torch.empty((), dtype=torch.float64, device=p.device) if pq else None
+        check(lib().tsn_normal(self._h, pp, sp, dp, float(lam), qp, tp, None if d is None else d.data_ptr(),
+                               _stream_handle(stream)))
+        return out, t, d
+
+    def rdot(self, a, b, stream=None):
+        """Re <a, b> over two complex64 device tensors of one size, FP64 in a fixed order
+        (tsn_rdot): a 0-d FP64 tensor on the device (no sync)."""
+        torch = _torch()
+        if a.numel() != b.numel():
+            raise ValueError("rdot needs two tensors of one size")
+        ap = _dev_ptr(a, torch.complex64, tuple(a.shape), "a")
+        bp = _dev_ptr(b, torch.complex64, tuple(b.shape), "b")
+        d = torch.empty((), dtype=torch.float64, device=a.device)
+        check(lib().tsn_rdot(self._h, ap, bp, int(a.numel()), d.data_ptr(), _stream_handle(stream)))
+        return d
 
     def cg_sense(self, y, smaps, *, density=None, lam=1e-4, iters=10, operator_scale=1.0, out=None, stream=None,
                  sync=True, reliable_update_period=0, reliable_update_direction="restart",
