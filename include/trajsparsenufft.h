@@ -225,6 +225,23 @@ tsn_status tsn_normal(tsn_plan* plan, const void* p, const void* smaps, const fl
                       void* q, void* coil_images, double* pq, tsn_stream_t stream);
 tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, double* out,
                     tsn_stream_t stream);
+/* One reverse-mode CG step (the adjoint of alpha = rho / gamma, x' = x + alpha p, r' = r -
+ * alpha q, rho' = |r'|^2, p' = r' + (rho'/rho) p with q = M p, gamma = Re <p, q>) for
+ * differentiable unrolled solves; no counterpart in the reference, which has no gradients.
+ * Device scalars (FP64): rho, rho_next = rho', gamma, rhob (cotangent of rho'); rhob_out
+ * receives the cotangent of rho.  Vectors of n complex64: rb, pb (cotangents of r', p') are
+ * updated in place to r-bar of this step and to p-bar minus M qb; qb receives the cotangent
+ * of q; p, q, r_next = r', xb (cotangent of x') are read.  Five FP64 inner products come
+ * from one pass before any vector changes.  tsn_cg_adjoint_finish then adds M qb (mqb) to
+ * pb and, with sb != NULL, adds conj(qb) t_c + tb_c conj(p) to the coil-map cotangent sb
+ * [coils][n] (t = coil images of M p, tb = those of M qb, as tsn_normal returns them). */
+tsn_status tsn_cg_adjoint_step(tsn_plan* plan, int64_t n, const double* rho, const double* rho_next,
+                               const double* gamma, const double* rhob, double* rhob_out, void* rb,
+                               void* pb, const void* p, const void* q, const void* r_next,
+                               const void* xb, void* qb, tsn_stream_t stream);
+tsn_status tsn_cg_adjoint_finish(tsn_plan* plan, int64_t n, int32_t coils, void* pb, const void* mqb,
+                                 const void* qb, const void* coil_images, const void* coil_images_bar,
+                                 const void* p, void* sb, tsn_stream_t stream);
 /* The FP32-class operators of a plan built with TSN_FLAG_REFERENCE_STEPS (the reference's
  * forward_reference / adjoint_reference, reference_sparse_solver.py:590-630, which its CG uses
  * for scheduled reference steps): same arguments and units as tsn_forward / tsn_adjoint, every

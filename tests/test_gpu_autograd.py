@@ -210,3 +210,43 @@ def test_normal_operator_and_fp64_dots_in_cuda():
     assert abs(float(d.cpu()) - want) <= 1e-12 * abs(want)
     with pytest.raises(ValueError):
         plan.rdot(pt.conj(), q)
+
+
+class _ComposedOps:
+    """PlanOps without its fused pieces: autograd._Sense then composes the SENSE algebra, the
+    inner products and the reverse CG recurrences from the coil operators with torch."""
+
+    def __init__(self, plan):
+        self.plan = plan
+
+    def forward_coils(self, ci):
+        return self.plan.forward(ci.contiguous())
+
+    def adjoint_coils(self, y):
+        return self.plan.adjoint(y.contiguous())
+
+
+def test_fused_backward_matches_composed_backward():
+    """The gradients through the plan's kernels (tsn_normal, tsn_rdot, tsn_cg_adjoint_step /
+    _finish) against the same unrolled CG composed with torch from the coil operators, at the
+    grad4 shape with density weights and a nonzero x0. Gate: 1e-3 relative per input (the two
+    paths round the FP16x2 panels differently and the 10-iteration CG amplifies it; the FD
+    checks hold both to the FP64 truth at the same 1e-3)."""
+    from trajsparsenufft_b200 import autograd as tad
+    from trajsparsenufft_b200 import synth
+    from trajsparsenufft_b200.operator import Plan
+    traj, x, s, n, g, c, j, readout = case("grad4")
+    y = measurement("grad4")
+    w = torch.from_numpy(synth.ramp_density(traj, readout).astype(np.float32)).cuda()
+    rng = np.random.default_rng(23)
+    x0 = (0.1 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
+    plan = Plan.from_trajectory(traj, im_size=n, grid_size=g, coils=c, width=j)
+    xt = torch.from_numpy(x).cuda()
+    grads = []
+    for ops in (tad.PlanOps(plan), _ComposedOps(plan)):
+        leaves = [torch.from_numpy(a.astype(np.complex64)).cuda().requires_grad_(True) for a in (y, s, x0)]
+        xk = tad.cg_sense(leaves[0], leaves[1], ops, x0=leaves[2], density=w, lam=LAM, iters=ITERS, checkpoint=2)
+        (xk - xt).abs().pow(2).sum().backward()
+        grads.append([t.grad.cpu().numpy() for t in leaves])
+    for a, b in zip(*grads):
+        assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(b)

@@ -56,6 +56,14 @@ class PlanOps:
         """F(S_c x) with the SENSE expansion inside the row transforms (tsn_forward)."""
         return self.plan.forward(x.contiguous(), smaps.contiguous())
 
+    def adjoint_step(self, rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb):
+        """Reverse-mode CG step in the plan's kernels (rb, pb in place): (qb, rhob of the step)."""
+        return self.plan.cg_adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb)
+
+    def adjoint_finish(self, pb, mqb, qb=None, t=None, tb=None, p=None, sb=None):
+        """pb += M qb and the coil-map cotangent update, in place."""
+        self.plan.cg_adjoint_finish(pb, mqb, qb, t, tb, p, sb)
+
 
 def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
     """Re <a, b> = sum(a.re b.re + a.im b.im), accumulated in FP64 (a 0-d tensor), like the graph
@@ -72,7 +80,7 @@ class _Sense:
 
     def __init__(self, ops, smaps, density, lam):
         self.ops, self.s, self.w, self.lam = ops, smaps, density, lam
-        self.fused = all(hasattr(ops, k) for k in ("normal", "rdot", "forward_maps"))
+        self.fused = all(hasattr(ops, k) for k in ("normal", "rdot", "forward_maps", "adjoint_step", "adjoint_finish"))
 
     def weigh(self, y):
         return y if self.w is None else y * self.w
@@ -211,9 +219,9 @@ class UnrolledCgSense(torch.autograd.Function):
         S = _Sense(ctx.ops, smaps, density, ctx.lam)
         need_y, need_s, need_x0 = ctx.needs_input_grad[0], ctx.needs_input_grad[1], ctx.needs_input_grad[2]
         c, iters = ctx.checkpoint, ctx.iters
-        xb = gx
-        rb = torch.zeros_like(gx)
-        pb = torch.zeros_like(gx)
+        xb = gx.contiguous()
+        rb = torch.zeros_like(xb)
+        pb = torch.zeros_like(xb)
         rhob = torch.zeros((), dtype=torch.float64, device=gx.device)
         sb = torch.zeros_like(smaps) if need_s else None
         for seg in reversed(range(len(cps))):
@@ -236,6 +244,14 @@ class UnrolledCgSense(torch.autograd.Function):
                 p = r_n + beta * p
                 r, rho = r_n, rho_n
             for p, q, t, r_n, rho, rho_n, gamma, alpha, beta in reversed(steps):
+                if S.fused:  # the same recurrences in the plan's kernels (rb, pb, sb in place)
+                    qb, rhob = ctx.ops.adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb)
+                    if need_s:
+                        mqb, tb = S.M_coils(qb)
+                        ctx.ops.adjoint_finish(pb, mqb, qb, t, tb, p, sb)
+                    else:
+                        ctx.ops.adjoint_finish(pb, S.M(qb))
+                    continue
                 rb = rb + pb                                   # p' = r' + beta p
                 betab = S.dot(pb, p)
                 pbk = beta * pb

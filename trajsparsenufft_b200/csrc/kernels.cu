@@ -1461,6 +1461,127 @@ void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_
   sum_partials_to_kernel<<<1, 256, 0, s>>>(parts, n, out);
 }
 
+// ---- reverse-mode CG step (the adjoint recurrences of one CG iteration) -------------------
+// Forward step k: alpha = rho / gamma (gamma = Re <p, q>, q = M p), x' = x + alpha p,
+// r' = r - alpha q, rho' = |r'|^2, beta = rho' / rho, p' = r' + beta p. Given the cotangents
+// xb (of x', constant over the solve), rb (of r'), pb (of p'), rhob (of rho'), the step makes
+//   rb2   = rb + pb + 2 rhob_n r'                 rhob_n = rhob + <pb, p> / rho
+//   alphab = <xb, p> - <rb2, q>                   gammab = -alphab rho / gamma^2
+//   qb    = -alpha rb2 + gammab p
+//   pbk   = beta pb + alpha xb + gammab q         (pb of step k = pbk + M qb, added later)
+//   rhobk = -<pb, p> rho' / rho^2 + alphab / gamma
+// with <rb2, q> = <rb, q> + <pb, q> + 2 rhob_n <r', q>, so the five FP64 inner products come
+// from one pass over the vectors before any of them changes.
+constexpr int kCgbBlocks = 296;  // 2 x 148 SMs
+
+__global__ void cgb_dots_kernel(int64_t n, const float2* __restrict__ rb, const float2* __restrict__ pb,
+                                const float2* __restrict__ p, const float2* __restrict__ q,
+                                const float2* __restrict__ rn, const float2* __restrict__ xb,
+                                double* __restrict__ parts) {
+  __shared__ double red[165];
+  double d[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 vpb = pb[i], vp = p[i], vq = q[i], vrb = rb[i], vrn = rn[i], vxb = xb[i];
+    d[0] += static_cast<double>(vpb.x) * vp.x + static_cast<double>(vpb.y) * vp.y;
+    d[1] += static_cast<double>(vrb.x) * vq.x + static_cast<double>(vrb.y) * vq.y;
+    d[2] += static_cast<double>(vpb.x) * vq.x + static_cast<double>(vpb.y) * vq.y;
+    d[3] += static_cast<double>(vrn.x) * vq.x + static_cast<double>(vrn.y) * vq.y;
+    d[4] += static_cast<double>(vxb.x) * vp.x + static_cast<double>(vxb.y) * vp.y;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const double v = warp_sum(d[k]);
+    if (lane == 0) red[33 * k + warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[33 * threadIdx.x + w];
+    parts[static_cast<int64_t>(threadIdx.x) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// sc (device FP64): [0] rho, [1] rho', [2] gamma, [3] rhob in; [4] rhob of step k out.
+__global__ void cgb_update_kernel(int64_t n, int nparts, const double* __restrict__ parts,
+                                  const double* __restrict__ rho_p, const double* __restrict__ rhon_p,
+                                  const double* __restrict__ gamma_p, const double* __restrict__ rhob_p,
+                                  double* __restrict__ rhob_out, float2* __restrict__ rb, float2* __restrict__ pb,
+                                  const float2* __restrict__ p, const float2* __restrict__ q,
+                                  const float2* __restrict__ rn, const float2* __restrict__ xb,
+                                  float2* __restrict__ qb) {
+  __shared__ double red[132];
+  __shared__ double dl[5];
+  const double4 s4 = sum_partials4(parts, nparts, nparts, red);
+  if (threadIdx.x == 0) {
+    dl[0] = s4.x;
+    dl[1] = s4.y;
+    dl[2] = s4.z;
+    dl[3] = s4.w;
+  }
+  const double d5 = sum_partials(parts + 4 * static_cast<int64_t>(nparts), nparts, red);
+  __syncthreads();
+  const double rho = *rho_p, rho_n = *rhon_p, gamma = *gamma_p, rhob = *rhob_p;
+  const double alpha = rho / gamma, beta = rho_n / rho;
+  const double betab = dl[0];
+  const double rhob_n = rhob + betab / rho;
+  const double rb2q = dl[1] + dl[2] + 2.0 * rhob_n * dl[3];
+  const double alphab = d5 - rb2q;
+  const double gammab = -alphab * rho / (gamma * gamma);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rhob_out = -betab * rho_n / (rho * rho) + alphab / gamma;
+  const float a = static_cast<float>(alpha), b = static_cast<float>(beta), g = static_cast<float>(gammab),
+              h = static_cast<float>(2.0 * rhob_n);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 vrb = rb[i], vpb = pb[i], vp = p[i], vq = q[i], vrn = rn[i], vxb = xb[i];
+    const float2 r2 = make_float2(vrb.x + vpb.x + h * vrn.x, vrb.y + vpb.y + h * vrn.y);
+    rb[i] = r2;
+    qb[i] = make_float2(-a * r2.x + g * vp.x, -a * r2.y + g * vp.y);
+    pb[i] = make_float2(b * vpb.x + a * vxb.x + g * vq.x, b * vpb.y + a * vxb.y + g * vq.y);
+  }
+}
+
+// pb += M qb; with sb given, sb[c] += conj(qb) t[c] + tb[c] conj(p) over `coils` planes of n.
+__global__ void cgb_finish_kernel(int64_t n, int coils, float2* __restrict__ pb, const float2* __restrict__ mqb,
+                                  const float2* __restrict__ qb, const float2* __restrict__ t,
+                                  const float2* __restrict__ tb, const float2* __restrict__ p,
+                                  float2* __restrict__ sb) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 vm = mqb[i];
+    float2 vpb = pb[i];
+    vpb.x += vm.x;
+    vpb.y += vm.y;
+    pb[i] = vpb;
+    if (!sb) continue;
+    const float2 vq = qb[i], vp = p[i];
+    for (int c = 0; c < coils; ++c) {
+      const size_t j = static_cast<size_t>(c) * n + i;
+      const float2 vt = t[j], vtb = tb[j];
+      float2 acc = sb[j];
+      // conj(qb) t + tb conj(p)
+      acc.x += vq.x * vt.x + vq.y * vt.y + vtb.x * vp.x + vtb.y * vp.y;
+      acc.y += vq.x * vt.y - vq.y * vt.x + vtb.y * vp.x - vtb.x * vp.y;
+      sb[j] = acc;
+    }
+  }
+}
+
+void launch_cg_adjoint_step(int64_t n, double* parts, const double* rho, const double* rho_n, const double* gamma,
+                            const double* rhob, double* rhob_out, float2* rb, float2* pb, const float2* p,
+                            const float2* q, const float2* rn, const float2* xb, float2* qb, cudaStream_t s) {
+  cgb_dots_kernel<<<kCgbBlocks, 256, 0, s>>>(n, rb, pb, p, q, rn, xb, parts);
+  cgb_update_kernel<<<kCgbBlocks, 256, 0, s>>>(n, kCgbBlocks, parts, rho, rho_n, gamma, rhob, rhob_out, rb, pb, p, q,
+                                                rn, xb, qb);
+}
+
+void launch_cg_adjoint_finish(int64_t n, int coils, float2* pb, const float2* mqb, const float2* qb, const float2* t,
+                              const float2* tb, const float2* p, float2* sb, cudaStream_t s) {
+  cgb_finish_kernel<<<kCgbBlocks, 256, 0, s>>>(n, coils, pb, mqb, qb, t, tb, p, sb);
+}
+
 template <class T>
 __global__ void gather_rows_kernel(const T* __restrict__ src, const int32_t* __restrict__ map, int64_t rows, int width,
                                    T* __restrict__ dst) {

@@ -214,6 +214,14 @@ void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters
 void launch_rdot(const float2* a, const float2* b, int64_t n, double* parts, double* out, cudaStream_t s);
 // out[0] = the sum of n partials in a fixed order
 void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_t s);
+// Reverse-mode CG step (kernels.cu): five FP64 inner products in one pass (parts: 5 x 296
+// doubles), then rb, pb updated in place, qb written and rhob of the step to *rhob_out.
+void launch_cg_adjoint_step(int64_t n, double* parts, const double* rho, const double* rho_n, const double* gamma,
+                            const double* rhob, double* rhob_out, float2* rb, float2* pb, const float2* p,
+                            const float2* q, const float2* rn, const float2* xb, float2* qb, cudaStream_t s);
+// pb += mqb and, with sb given, the coil-map cotangent sb[c] += conj(qb) t[c] + tb[c] conj(p).
+void launch_cg_adjoint_finish(int64_t n, int coils, float2* pb, const float2* mqb, const float2* qb, const float2* t,
+                              const float2* tb, const float2* p, float2* sb, cudaStream_t s);
 
 void launch_gather_rows_f16(const __half* src, const int32_t* map, int64_t rows, int width, __half* dst,
                             cudaStream_t s);

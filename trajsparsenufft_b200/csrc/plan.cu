@@ -119,6 +119,7 @@ struct tsn_plan {
   int64_t M = 0;
   DevView view[2];
   DeviceBuffer scaling, tw, z1, z2, panel, spanel, grid, r, p, ap, rhs, parts_pap, parts_rr, norm_parts, state;
+  DeviceBuffer adj_parts;  // 5 x 296 FP64 partials of the reverse-mode CG step
   tsn_plan_info info{};
   std::map<GraphKey, cudaGraphExec_t> graphs;
   ~tsn_plan() {
@@ -573,6 +574,7 @@ void allocate_workspaces(tsn_plan* P) {
   P->norm_parts.alloc(sizeof(double) * kNormParts);
   P->state.alloc(sizeof(CgState));
   CUDA_OK(cudaMemset(P->state.ptr, 0, sizeof(CgState)));
+  P->adj_parts.alloc(sizeof(double) * 5 * 296);
   P->info.dims = P->dims;
   P->info.workspace_bytes = static_cast<int64_t>(P->z1.bytes + P->z2.bytes + P->panel.bytes + P->spanel.bytes +
                                                  P->grid.bytes + 4 * P->r.bytes + P->state.bytes);
@@ -1292,6 +1294,46 @@ tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, dou
     CUDA_OK(cudaSetDevice(plan->desc.device));
     launch_rdot(static_cast<const float2*>(a), static_cast<const float2*>(b), n, plan->norm_parts.as<double>(), out,
                 reinterpret_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_cg_adjoint_step(tsn_plan* plan, int64_t n, const double* rho, const double* rho_next,
+                               const double* gamma, const double* rhob, double* rhob_out, void* rb, void* pb,
+                               const void* p, const void* q, const void* r_next, const void* xb, void* qb,
+                               tsn_stream_t stream) {
+  try {
+    if (!plan || !rho || !rho_next || !gamma || !rhob || !rhob_out || !rb || !pb || !p || !q || !r_next || !xb || !qb)
+      fail(TSN_ERR_ARG, "NULL argument");
+    if (n < 0) fail(TSN_ERR_ARG, "n must be >= 0");
+    CUDA_OK(cudaSetDevice(plan->desc.device));
+    launch_cg_adjoint_step(n, plan->adj_parts.as<double>(), rho, rho_next, gamma, rhob, rhob_out,
+                           static_cast<float2*>(rb), static_cast<float2*>(pb), static_cast<const float2*>(p),
+                           static_cast<const float2*>(q), static_cast<const float2*>(r_next),
+                           static_cast<const float2*>(xb), static_cast<float2*>(qb),
+                           reinterpret_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
+tsn_status tsn_cg_adjoint_finish(tsn_plan* plan, int64_t n, int32_t coils, void* pb, const void* mqb, const void* qb,
+                                 const void* coil_images, const void* coil_images_bar, const void* p, void* sb,
+                                 tsn_stream_t stream) {
+  try {
+    if (!plan || !pb || !mqb) fail(TSN_ERR_ARG, "NULL argument");
+    if (n < 0 || coils < 0) fail(TSN_ERR_ARG, "n and coils must be >= 0");
+    if (sb && (!qb || !coil_images || !coil_images_bar || !p)) fail(TSN_ERR_ARG, "the map cotangent needs qb, t, tb and p");
+    CUDA_OK(cudaSetDevice(plan->desc.device));
+    launch_cg_adjoint_finish(n, coils, static_cast<float2*>(pb), static_cast<const float2*>(mqb),
+                             static_cast<const float2*>(qb), static_cast<const float2*>(coil_images),
+                             static_cast<const float2*>(coil_images_bar), static_cast<const float2*>(p),
+                             static_cast<float2*>(sb), reinterpret_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
     return TSN_OK;
   } catch (const std::exception& e) {

@@ -221,6 +221,39 @@ class Plan:
         check(lib().tsn_rdot(self._h, ap, bp, int(a.numel()), d.data_ptr(), _stream_handle(stream)))
         return d
 
+    def cg_adjoint_step(self, rho, rho_next, gamma, rhob, rb, pb, p, q, r_next, xb, stream=None):
+        """One reverse-mode CG step (tsn_cg_adjoint_step): rb and pb (complex64, one image each)
+        are updated in place; returns (qb, the cotangent of rho as a 0-d FP64 device tensor).
+        rho, rho_next, gamma, rhob are 0-d FP64 device tensors."""
+        torch = _torch()
+        shape = tuple(p.shape)
+        ptrs = [_dev_ptr(v, torch.float64, (), nm) for v, nm in
+                ((rho, "rho"), (rho_next, "rho_next"), (gamma, "gamma"), (rhob, "rhob"))]
+        vec = [_dev_ptr(v, torch.complex64, shape, nm) for v, nm in
+               ((rb, "rb"), (pb, "pb"), (p, "p"), (q, "q"), (r_next, "r_next"), (xb, "xb"))]
+        qb = torch.empty(shape, dtype=torch.complex64, device=p.device)
+        rhob_out = torch.empty((), dtype=torch.float64, device=p.device)
+        check(lib().tsn_cg_adjoint_step(self._h, int(p.numel()), *ptrs, C.c_void_p(rhob_out.data_ptr()), *vec,
+                                        C.c_void_p(qb.data_ptr()), _stream_handle(stream)))
+        return qb, rhob_out
+
+    def cg_adjoint_finish(self, pb, mqb, qb=None, t=None, tb=None, p=None, sb=None, stream=None):
+        """pb += mqb in place and, with sb given, sb[c] += conj(qb) t[c] + tb[c] conj(p)
+        (tsn_cg_adjoint_finish)."""
+        torch = _torch()
+        shape = tuple(pb.shape)
+        cf = torch.complex64
+        args = [_dev_ptr(pb, cf, shape, "pb"), _dev_ptr(mqb, cf, shape, "mqb")]
+        if sb is None:
+            args += [None, None, None, None, None]
+            coils = 0
+        else:
+            cshape = tuple(sb.shape)
+            coils = cshape[0]
+            args += [_dev_ptr(qb, cf, shape, "qb"), _dev_ptr(t, cf, cshape, "t"), _dev_ptr(tb, cf, cshape, "tb"),
+                     _dev_ptr(p, cf, shape, "p"), _dev_ptr(sb, cf, cshape, "sb")]
+        check(lib().tsn_cg_adjoint_finish(self._h, int(pb.numel()), int(coils), *args, _stream_handle(stream)))
+
     def cg_sense(self, y, smaps, *, density=None, lam=1e-4, iters=10, operator_scale=1.0, out=None, stream=None,
                  sync=True, reliable_update_period=0, reliable_update_direction="restart",
                  scheduled_reference_period=0, reference_steps=()):
