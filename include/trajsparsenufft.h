@@ -225,6 +225,14 @@ tsn_status tsn_normal(tsn_plan* plan, const void* p, const void* smaps, const fl
                       void* q, void* coil_images, double* pq, tsn_stream_t stream);
 tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, double* out,
                     tsn_stream_t stream);
+/* One CG step on caller-owned vectors (the update of reference_sparse_solver.py:288-332
+ * cg_sense for callers that keep their own states): alpha = *rho / *gamma; x_out = x + alpha p
+ * (x and x_out may both be NULL); r_out = r - alpha q; *rho_out = |r_out|^2 in FP64 (fixed
+ * order); p_out = r_out + (*rho_out / *rho) p.  Scalars are device doubles, vectors n complex64
+ * on the device; outputs must not alias inputs. */
+tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const double* gamma, const void* x,
+                       const void* p, const void* r, const void* q, void* x_out, void* r_out,
+                       void* p_out, double* rho_out, tsn_stream_t stream);
 /* One reverse-mode CG step (the adjoint of alpha = rho / gamma, x' = x + alpha p, r' = r -
  * alpha q, rho' = |r'|^2, p' = r' + (rho'/rho) p with q = M p, gamma = Re <p, q>) for
  * differentiable unrolled solves; no counterpart in the reference, which has no gradients.

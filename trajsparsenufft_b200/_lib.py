@@ -30,7 +30,7 @@ EXPORTED = (
     "tsn_version", "tsn_get_last_error_string", "tsn_plan_desc_default", "tsn_kb_interpolation_csr",
     "tsn_kb_deapodization", "tsn_kb_weights_csr3", "tsn_kb_deapodization3", "tsn_pack_csr_to_dirs", "tsn_pack_view_tiles", "tsn_export_view_dir",
     "tsn_plan_create_from_pack", "tsn_plan_create_from_trajectory", "tsn_plan_destroy", "tsn_plan_get_info",
-    "tsn_forward", "tsn_adjoint", "tsn_forward_reference", "tsn_adjoint_reference", "tsn_normal", "tsn_rdot", "tsn_cg_adjoint_step", "tsn_cg_adjoint_finish", "tsn_cg_sense", "tsn_cg_sense_ex", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
+    "tsn_forward", "tsn_adjoint", "tsn_forward_reference", "tsn_adjoint_reference", "tsn_normal", "tsn_rdot", "tsn_cg_step", "tsn_cg_adjoint_step", "tsn_cg_adjoint_finish", "tsn_cg_sense", "tsn_cg_sense_ex", "tsn_batch_create", "tsn_batch_destroy", "tsn_batch_cg_sense",
     "tsn_fft_forward_panel", "tsn_fft_adjoint_image", "tsn_profile_stages", "tsn_fft_adjoint_image_static",
     "tsn_interp_component",
 )
@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         "tsn_forward_reference": (C.c_int, [P, P, P, P, P]),
         "tsn_normal": (C.c_int, [P, P, P, P, C.c_float, P, P, P, P]),
         "tsn_rdot": (C.c_int, [P, P, P, C.c_int64, P, P]),
+        "tsn_cg_step": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P]),
         "tsn_cg_adjoint_step": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P]),
         "tsn_cg_adjoint_finish": (C.c_int, [P, C.c_int64, C.c_int32, P, P, P, P, P, P, P, P]),
         "tsn_adjoint_reference": (C.c_int, [P, P, P, P, P]),

@@ -56,6 +56,11 @@ class PlanOps:
         """F(S_c x) with the SENSE expansion inside the row transforms (tsn_forward)."""
         return self.plan.forward(x.contiguous(), smaps.contiguous())
 
+    def step(self, rho, gamma, x, p, r, q):
+        """One CG step in the plan's kernels: (x' or None, r', p', rho')."""
+        return self.plan.cg_step(rho, gamma, None if x is None else x.contiguous(), p.contiguous(), r.contiguous(),
+                                 q.contiguous())
+
     def adjoint_step(self, rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb):
         """Reverse-mode CG step in the plan's kernels (rb, pb in place): (qb, rhob of the step)."""
         return self.plan.cg_adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb)
@@ -80,7 +85,8 @@ class _Sense:
 
     def __init__(self, ops, smaps, density, lam):
         self.ops, self.s, self.w, self.lam = ops, smaps, density, lam
-        self.fused = all(hasattr(ops, k) for k in ("normal", "rdot", "forward_maps", "adjoint_step", "adjoint_finish"))
+        self.fused = all(hasattr(ops, k) for k in ("normal", "rdot", "forward_maps", "step", "adjoint_step",
+                                                   "adjoint_finish"))
 
     def weigh(self, y):
         return y if self.w is None else y * self.w
@@ -110,6 +116,24 @@ class _Sense:
             return q, pq
         q = self.M(p)
         return q, _rdot(p, q)
+
+    def M_coils_dot(self, p):
+        """(M p, the coil images G(S p), Re <p, M p>)."""
+        if self.fused:
+            return self.ops.normal(p, self.s, self.w, self.lam, coils=True, pq=True)
+        q, t = self.M_coils(p)
+        return q, t, _rdot(p, q)
+
+    def step(self, rho, gamma, x, p, r, q):
+        """CG step: (x + alpha p or None, r' = r - alpha q, p' = r' + (rho'/rho) p, rho' = |r'|^2)
+        with alpha = rho / gamma."""
+        if self.fused:
+            return self.ops.step(rho, gamma, x, p, r, q)
+        alpha = rho / gamma
+        x_n = None if x is None else x + alpha * p
+        r_n = r - alpha * q
+        rho_n = _rdot(r_n, r_n)
+        return x_n, r_n, r_n + (rho_n / rho) * p, rho_n
 
     def M_coils(self, p):
         """(M p, the coil images G(S p)) — the second feeds the coil-map gradient."""
@@ -183,19 +207,13 @@ class UnrolledCgSense(torch.autograd.Function):
         firsts = []   # q = M p (and the coil images G(S p) when maps need gradients) of each
         for k in range(iters):   # checkpointed step: the backward reuses them instead of recomputing
             if k % checkpoint == 0 and need_s:
-                q, t = S.M_coils(p)
+                q, t, gamma = S.M_coils_dot(p)
                 firsts.append((q, t))
-                gamma = S.dot(p, q)
             else:
                 q, gamma = S.M_dot(p)
                 if k % checkpoint == 0:
                     firsts.append((q,))
-            alpha = rho / gamma
-            x = x + alpha * p
-            r = r - alpha * q
-            rho_n = S.dot(r, r)
-            p = r + (rho_n / rho) * p
-            rho = rho_n
+            x, r, p, rho = S.step(rho, gamma, x, p, r, q)
             if (k + 1) % checkpoint == 0 and k + 1 < iters:
                 cps.append((x, r, p, rho))
         ctx.ops, ctx.lam, ctx.iters, ctx.checkpoint, ctx.x0_zero = ops, lam, iters, checkpoint, x0_zero
@@ -236,12 +254,10 @@ class UnrolledCgSense(torch.autograd.Function):
                 else:
                     q, t = S.M(p), None
                 gamma = S.dot(p, q)
-                alpha = rho / gamma
-                r_n = r - alpha * q
-                rho_n = S.dot(r_n, r_n)
-                beta = rho_n / rho
-                steps.append((p, q, t, r_n, rho, rho_n, gamma, alpha, beta))
-                p = r_n + beta * p
+                _, r_n, p_n, rho_n = S.step(rho, gamma, None, p, r, q)
+                ab = (None, None) if S.fused else (rho / gamma, rho_n / rho)  # alpha, beta: composed path
+                steps.append((p, q, t, r_n, rho, rho_n, gamma, *ab))
+                p = p_n
                 r, rho = r_n, rho_n
             for p, q, t, r_n, rho, rho_n, gamma, alpha, beta in reversed(steps):
                 if S.fused:  # the same recurrences in the plan's kernels (rb, pb, sb in place)

@@ -1569,6 +1569,53 @@ __global__ void cgb_finish_kernel(int64_t n, int coils, float2* __restrict__ pb,
   }
 }
 
+// ---- one forward CG step on caller-owned vectors (differentiable solves) ------------------
+// alpha = rho / gamma; x' = x + alpha p (when x is given); r' = r - alpha q; rho' = |r'|^2
+// (FP64, fixed order); p' = r' + (rho' / rho) p. Outputs are separate arrays.
+__global__ void cgf_update_kernel(int64_t n, const double* __restrict__ rho_p, const double* __restrict__ gamma_p,
+                                  const float2* __restrict__ x, const float2* __restrict__ p,
+                                  const float2* __restrict__ r, const float2* __restrict__ q,
+                                  float2* __restrict__ x_out, float2* __restrict__ r_out, double* __restrict__ parts) {
+  __shared__ double red[33];
+  const float a = static_cast<float>(*rho_p / *gamma_p);
+  double acc = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 vp = p[i], vr = r[i], vq = q[i];
+    if (x) {
+      const float2 vx = x[i];
+      x_out[i] = make_float2(vx.x + a * vp.x, vx.y + a * vp.y);
+    }
+    const float2 rn = make_float2(vr.x - a * vq.x, vr.y - a * vq.y);
+    r_out[i] = rn;
+    acc += static_cast<double>(rn.x) * rn.x + static_cast<double>(rn.y) * rn.y;
+  }
+  const double t = block_sum(acc, red);
+  if (threadIdx.x == 0) parts[blockIdx.x] = t;
+}
+
+__global__ void cgf_direction_kernel(int64_t n, int nparts, const double* __restrict__ parts,
+                                     const double* __restrict__ rho_p, double* __restrict__ rho_out,
+                                     const float2* __restrict__ p, const float2* __restrict__ r_new,
+                                     float2* __restrict__ p_out) {
+  __shared__ double red[33];
+  const double rho_n = sum_partials(parts, nparts, red);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rho_out = rho_n;
+  const float b = static_cast<float>(rho_n / *rho_p);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 vp = p[i], vr = r_new[i];
+    p_out[i] = make_float2(vr.x + b * vp.x, vr.y + b * vp.y);
+  }
+}
+
+void launch_cg_step(int64_t n, double* parts, const double* rho, const double* gamma, const float2* x, const float2* p,
+                    const float2* r, const float2* q, float2* x_out, float2* r_out, float2* p_out, double* rho_out,
+                    cudaStream_t s) {
+  cgf_update_kernel<<<kCgbBlocks, 256, 0, s>>>(n, rho, gamma, x, p, r, q, x_out, r_out, parts);
+  cgf_direction_kernel<<<kCgbBlocks, 256, 0, s>>>(n, kCgbBlocks, parts, rho, rho_out, p, r_out, p_out);
+}
+
 void launch_cg_adjoint_step(int64_t n, double* parts, const double* rho, const double* rho_n, const double* gamma,
                             const double* rhob, double* rhob_out, float2* rb, float2* pb, const float2* p,
                             const float2* q, const float2* rn, const float2* xb, float2* qb, cudaStream_t s) {

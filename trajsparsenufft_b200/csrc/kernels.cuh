@@ -214,6 +214,12 @@ void launch_cg_finish(int nparts, const double* rr_parts, CgState* st, int iters
 void launch_rdot(const float2* a, const float2* b, int64_t n, double* parts, double* out, cudaStream_t s);
 // out[0] = the sum of n partials in a fixed order
 void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_t s);
+// Forward CG step on caller-owned vectors: alpha = rho / gamma, x_out = x + alpha p (x may be
+// null), r_out = r - alpha q, rho_out = |r_out|^2 (FP64, 296 partials in parts, fixed order),
+// p_out = r_out + (rho_out / rho) p.
+void launch_cg_step(int64_t n, double* parts, const double* rho, const double* gamma, const float2* x, const float2* p,
+                    const float2* r, const float2* q, float2* x_out, float2* r_out, float2* p_out, double* rho_out,
+                    cudaStream_t s);
 // Reverse-mode CG step (kernels.cu): five FP64 inner products in one pass (parts: 5 x 296
 // doubles), then rb, pb updated in place, qb written and rhob of the step to *rhob_out.
 void launch_cg_adjoint_step(int64_t n, double* parts, const double* rho, const double* rho_n, const double* gamma,

@@ -1301,6 +1301,25 @@ tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, dou
   }
 }
 
+tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const double* gamma, const void* x, const void* p,
+                       const void* r, const void* q, void* x_out, void* r_out, void* p_out, double* rho_out,
+                       tsn_stream_t stream) {
+  try {
+    if (!plan || !rho || !gamma || !p || !r || !q || !r_out || !p_out || !rho_out) fail(TSN_ERR_ARG, "NULL argument");
+    if ((x == nullptr) != (x_out == nullptr)) fail(TSN_ERR_ARG, "x and x_out go together");
+    if (n < 0) fail(TSN_ERR_ARG, "n must be >= 0");
+    CUDA_OK(cudaSetDevice(plan->desc.device));
+    launch_cg_step(n, plan->adj_parts.as<double>(), rho, gamma, static_cast<const float2*>(x),
+                   static_cast<const float2*>(p), static_cast<const float2*>(r), static_cast<const float2*>(q),
+                   static_cast<float2*>(x_out), static_cast<float2*>(r_out), static_cast<float2*>(p_out), rho_out,
+                   reinterpret_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TSN_OK;
+  } catch (const std::exception& e) {
+    return guard_status(e);
+  }
+}
+
 tsn_status tsn_cg_adjoint_step(tsn_plan* plan, int64_t n, const double* rho, const double* rho_next,
                                const double* gamma, const double* rhob, double* rhob_out, void* rb, void* pb,
                                const void* p, const void* q, const void* r_next, const void* xb, void* qb,

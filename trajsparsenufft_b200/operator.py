@@ -221,6 +221,22 @@ class Plan:
         check(lib().tsn_rdot(self._h, ap, bp, int(a.numel()), d.data_ptr(), _stream_handle(stream)))
         return d
 
+    def cg_step(self, rho, gamma, x, p, r, q, stream=None):
+        """One CG step on image vectors (tsn_cg_step): returns (x' or None, r', p', rho' as a
+        0-d FP64 device tensor) with alpha = rho / gamma; x may be None."""
+        torch = _torch()
+        shape = tuple(p.shape)
+        cf = torch.complex64
+        sc = [_dev_ptr(rho, torch.float64, (), "rho"), _dev_ptr(gamma, torch.float64, (), "gamma")]
+        xo = None if x is None else torch.empty(shape, dtype=cf, device=p.device)
+        ro, po = torch.empty(shape, dtype=cf, device=p.device), torch.empty(shape, dtype=cf, device=p.device)
+        rho_o = torch.empty((), dtype=torch.float64, device=p.device)
+        check(lib().tsn_cg_step(self._h, int(p.numel()), *sc, None if x is None else _dev_ptr(x, cf, shape, "x"),
+                                _dev_ptr(p, cf, shape, "p"), _dev_ptr(r, cf, shape, "r"), _dev_ptr(q, cf, shape, "q"),
+                                None if xo is None else C.c_void_p(xo.data_ptr()), C.c_void_p(ro.data_ptr()),
+                                C.c_void_p(po.data_ptr()), C.c_void_p(rho_o.data_ptr()), _stream_handle(stream)))
+        return xo, ro, po, rho_o
+
     def cg_adjoint_step(self, rho, rho_next, gamma, rhob, rb, pb, p, q, r_next, xb, stream=None):
         """One reverse-mode CG step (tsn_cg_adjoint_step): rb and pb (complex64, one image each)
         are updated in place; returns (qb, the cotangent of rho as a 0-d FP64 device tensor).
