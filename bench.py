@@ -71,6 +71,56 @@ def synth_inputs(cfg: dict, seed: int):
     return traj, x, s, w
 
 
+def nvml_handle(pynvml, index: int):
+    """NVML handle of CUDA device `index` (matched by UUID: NVML numbers every GPU of the
+    machine, CUDA only the visible ones)."""
+    import torch
+    uuid = str(torch.cuda.get_device_properties(index).uuid)
+    try:
+        return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+    except Exception:
+        return pynvml.nvmlDeviceGetHandleByIndex(index)
+
+
+def gpu_local_cpus(index: int) -> set:
+    """The CPUs NVML reports as local to CUDA device `index` (its NUMA node), within the ones
+    this process may use; empty when NVML cannot say."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        h = nvml_handle(pynvml, index)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, ((os.cpu_count() or 64) + 63) // 64)
+        cpus = {64 * i + b for i, w in enumerate(words) for b in range(64) if (int(w) >> b) & 1}
+        return cpus & os.sched_getaffinity(0)
+    except Exception:
+        return set()
+
+
+class NumaLocal:
+    """Allocates host buffers on the GPU's NUMA node: the calling thread runs on the GPU-local
+    CPUs inside the block, so the pinned pages it touches first land on that node, and the
+    copies to the device do not cross the inter-socket link. The thread's CPU set is restored
+    afterwards (the CPU baseline keeps every core)."""
+
+    def __init__(self, index: int):
+        self.cpus = gpu_local_cpus(index)
+        self.allowed = os.sched_getaffinity(0)
+
+    def __enter__(self):
+        if self.cpus and self.cpus != self.allowed:
+            os.sched_setaffinity(0, self.cpus)
+        return self
+
+    def __exit__(self, *exc):
+        if self.cpus and self.cpus != self.allowed:
+            os.sched_setaffinity(0, self.allowed)
+        return False
+
+    def summary(self) -> dict:
+        return {"gpu_local_cpus": len(self.cpus), "allowed_cpus": len(self.allowed),
+                "pinned_on_gpu_node": bool(self.cpus)}
+
+
 class ClockSampler:
     """Samples SM clock and throttle reasons through NVML while the timed region runs."""
 
@@ -88,7 +138,7 @@ class ClockSampler:
             import pynvml
             pynvml.nvmlInit()
             self._nv = pynvml
-            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self._h = nvml_handle(pynvml, index)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
         except Exception:
             self._nv = None
@@ -264,9 +314,11 @@ def run_ours(args, cfg) -> dict:
     # from pinned host memory and reads its image back.  The copy of step k+1 runs on a side
     # stream while step k solves (double-buffered device inputs); the L2 flush between steps
     # runs alone and its time is taken out of the total.
-    y_h = y.cpu().pin_memory()
-    s_h = smaps.cpu().pin_memory()
-    x_h = torch.empty(x_out.shape, dtype=x_out.dtype).pin_memory()
+    numa = NumaLocal(local)
+    with numa:
+        y_h = y.cpu().pin_memory()
+        s_h = smaps.cpu().pin_memory()
+        x_hb = [torch.empty(x_out.shape, dtype=x_out.dtype).pin_memory() for _ in range(2)]
     y_d = [torch.empty_like(y) for _ in range(2)]
     s_d = [torch.empty_like(smaps) for _ in range(2)]
     e2e_steps = max(3, args.steps // 2)
@@ -279,7 +331,6 @@ def run_ours(args, cfg) -> dict:
     # the image read-back is double-buffered too: step k's image leaves on a second side stream
     # while step k+1 solves (after that step's flush, which is taken out of the total)
     x_d = [x_out, torch.empty_like(x_out)]
-    x_hb = [x_h, torch.empty(x_out.shape, dtype=x_out.dtype).pin_memory()]
     down = torch.cuda.Stream(device=dev)
 
     def e2e_run(nsteps):
@@ -357,7 +408,8 @@ def run_ours(args, cfg) -> dict:
                 "overlap": "the input copy of step k+1 and the image read-back of step k-1 overlap the solve of step k",
                 "h2d_ms_per_step": round(h2d_ms, 4),
                 "repeats": [round(job_rate(world, 1, e2e_steps, m), 3) for m in e2e_repeats],
-                "statistic": f"median of {len(e2e_repeats)} runs of {e2e_steps} steps"},
+                "statistic": f"median of {len(e2e_repeats)} runs of {e2e_steps} steps",
+                "host_buffers": numa.summary()},
         "gpu_launches": args.steps * (5 + 6 * iters + 2),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -526,9 +578,10 @@ def run_batch(args, cfg) -> dict | None:
 
     # end to end: every step copies all cases' y and maps from pinned host memory (side stream,
     # overlapping the previous step's solve) and reads every image back
-    y_h = [y.cpu().pin_memory() for y in ys]
-    s_h = [s.cpu().pin_memory() for s in maps]
-    x_h = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
+    with NumaLocal(local):
+        y_h = [y.cpu().pin_memory() for y in ys]
+        s_h = [s.cpu().pin_memory() for s in maps]
+        x_h = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
     y_d = [[torch.empty_like(y) for y in ys] for _ in range(2)]
     s_d = [[torch.empty_like(s) for s in maps] for _ in range(2)]
     main = torch.cuda.current_stream()
@@ -745,10 +798,11 @@ def run_grad(args, cfg) -> dict | None:
 
     # end to end: inputs from pinned host memory into the graph's static inputs, then the loss
     # and every gradient back to the host
-    y_h = [y.cpu().pin_memory() for y in ys]
-    s_h = [s.cpu().pin_memory() for s in maps]
-    grads_h = [torch.empty(leaf.shape, dtype=leaf.dtype).pin_memory() for leaf in leaves]
-    loss_h = torch.empty((), dtype=g_loss.dtype).pin_memory()
+    with NumaLocal(local):
+        y_h = [y.cpu().pin_memory() for y in ys]
+        s_h = [s.cpu().pin_memory() for s in maps]
+        grads_h = [torch.empty(leaf.shape, dtype=leaf.dtype).pin_memory() for leaf in leaves]
+        loss_h = torch.empty((), dtype=g_loss.dtype).pin_memory()
 
     def e2e_step():
         for dst, h in zip(y_st + s_st, y_h + s_h):
@@ -947,9 +1001,10 @@ def run_volume(args, cfg) -> dict | None:
 
     # end to end with host buffers: y and maps in from pinned memory (next step's copy on a side
     # stream overlapping this step's solve), the volume back every step
-    y_h = y.cpu().pin_memory()
-    s_h = smaps.cpu().pin_memory()
-    x_h = torch.empty(x_out.shape, dtype=x_out.dtype).pin_memory()
+    with NumaLocal(local):
+        y_h = y.cpu().pin_memory()
+        s_h = smaps.cpu().pin_memory()
+        x_h = torch.empty(x_out.shape, dtype=x_out.dtype).pin_memory()
     y_d = [torch.empty_like(y) for _ in range(2)]
     s_d = [torch.empty_like(smaps) for _ in range(2)]
     main_s = torch.cuda.current_stream()

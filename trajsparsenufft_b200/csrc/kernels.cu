@@ -29,7 +29,10 @@ using namespace dev;
 // in the stream drains, and wait in pdl_wait before touching its results. Every kernel of the
 // CG iteration calls pdl_trigger once it has passed its own wait, so the interpolation behind
 // it may launch then. On the 256^2 / 8-coil headline solve this took a CG iteration from 71.8
-// to 69.5 us. The FFT stages are launched plainly: their CTAs, started early beside a kernel
+// to 69.5 us. Batched cases, whose kernels run side by side on slices of the GPU, launch it
+// plainly: early CTAs would wait beside the other cases' kernels (the 48-case batch measured
+// 1191 recons/s with it, 1325-1390 without it on other boxes; 1329 plain vs 1325 with every
+// launch plain on one box). The FFT stages are launched plainly: their CTAs, started early beside a kernel
 // that leaves room on the SMs (the row stages hold ~1.7 of 3 CTAs per SM; the interpolation
 // leaves room for one more), made the solve 3-9% slower although each stage timed alone
 // back to back got faster. They keep the same prologue split (plan rows before pdl_wait) for
@@ -377,7 +380,7 @@ static void launch_interp_s(const InterpView& v, const __half* panel, const Inte
   const size_t smem = static_cast<size_t>(kInterpWarps) * STAGES * (record_bytes(NCOMP) + 32 * ROWH * 2);
   auto k = interp_mmasp_kernel<ROWH, SPLIT, NCOMP, EPI, CONJ, STAGES, SUMC>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (blocks > 0) launch_k(k, blocks, kInterpWarps * 32, smem, s, true, v, panel, o);
+  if (blocks > 0) launch_k(k, blocks, kInterpWarps * 32, smem, s, v.programmatic != 0, v, panel, o);
 }
 
 template <int ROWH, bool SPLIT, int NCOMP, int EPI, bool CONJ, bool SUMC = false>

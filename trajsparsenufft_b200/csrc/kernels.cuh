@@ -69,6 +69,8 @@ struct InterpView {
   int32_t ncomp = 0;
   int32_t rec_bytes = 0;
   int32_t stages = 3;                   // per-warp ring depth: 3, or 4 when the gathered panel exceeds L2
+  int32_t programmatic = 1;             // 1: launched with programmatic dependent launch (0 for the
+                                        //    1/share slices of batched cases, which share the SMs)
   int32_t sum_components = 0;           // 1: the two components are a real coefficient's FP16 high and
                                         //    low parts, summed (else real / imaginary parts)
 };

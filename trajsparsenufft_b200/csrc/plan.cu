@@ -1095,6 +1095,7 @@ void prepare_share(tsn_plan* P, int share) {
     const std::vector<int2> ranges = cut_ranges(d.item_ends, d.tiles, warps);
     d.ranges_shared.upload(ranges);
     d.v_shared = d.v;
+    d.v_shared.programmatic = 0;  // slices of the GPU shared with other cases' kernels
     d.v_shared.warp_ranges = d.ranges_shared.as<int2>();
     d.v_shared.n_warps = static_cast<int32_t>(ranges.size());
     d.share = share;
