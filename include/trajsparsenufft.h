@@ -219,20 +219,28 @@ tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x
  * density W [M] may be NULL), with, when coil_images != NULL, the coil images
  * F^H W F(S_c p) [C][N][N] before the combine, and, when pq != NULL, Re <p, q> summed in FP64
  * in a fixed order into the device double *pq.  Same units as tsn_forward / tsn_adjoint.
+ * p_norm_parts (optional): n_p_norm_parts device doubles whose sum is |p|^2, such as the
+ * TSN_CG_STEP_PARTS partials tsn_cg_step writes for its p' (they set the FP16 panel scale;
+ * NULL: computed here by one more pass over p).
  * tsn_rdot: *out (device) = Re <a, b> = sum a.re b.re + a.im b.im over n complex values, FP64,
  * fixed order.  Both use the plan's workspaces: calls on one plan are ordered by their stream. */
 tsn_status tsn_normal(tsn_plan* plan, const void* p, const void* smaps, const float* density, float lambda,
-                      void* q, void* coil_images, double* pq, tsn_stream_t stream);
+                      void* q, void* coil_images, double* pq, const double* p_norm_parts,
+                      int32_t n_p_norm_parts, tsn_stream_t stream);
+/* Number of FP64 partials tsn_cg_step / tsn_cg_adjoint_step write to their optional
+ * p_norm_parts / qb_norm_parts outputs. */
+#define TSN_CG_STEP_PARTS 296
 tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, double* out,
                     tsn_stream_t stream);
 /* One CG step on caller-owned vectors (the update of reference_sparse_solver.py:288-332
  * cg_sense for callers that keep their own states): alpha = *rho / *gamma; x_out = x + alpha p
  * (x and x_out may both be NULL); r_out = r - alpha q; *rho_out = |r_out|^2 in FP64 (fixed
  * order); p_out = r_out + (*rho_out / *rho) p.  Scalars are device doubles, vectors n complex64
- * on the device; outputs must not alias inputs. */
+ * on the device; outputs must not alias inputs.  p_norm_parts (optional, TSN_CG_STEP_PARTS
+ * device doubles) receives partial sums of |p_out|^2 for the next tsn_normal. */
 tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const double* gamma, const void* x,
                        const void* p, const void* r, const void* q, void* x_out, void* r_out,
-                       void* p_out, double* rho_out, tsn_stream_t stream);
+                       void* p_out, double* rho_out, double* p_norm_parts, tsn_stream_t stream);
 /* One reverse-mode CG step (the adjoint of alpha = rho / gamma, x' = x + alpha p, r' = r -
  * alpha q, rho' = |r'|^2, p' = r' + (rho'/rho) p with q = M p, gamma = Re <p, q>) for
  * differentiable unrolled solves; no counterpart in the reference, which has no gradients.
@@ -242,11 +250,14 @@ tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const doubl
  * of q; p, q, r_next = r', xb (cotangent of x') are read.  Five FP64 inner products come
  * from one pass before any vector changes.  tsn_cg_adjoint_finish then adds M qb (mqb) to
  * pb and, with sb != NULL, adds conj(qb) t_c + tb_c conj(p) to the coil-map cotangent sb
- * [coils][n] (t = coil images of M p, tb = those of M qb, as tsn_normal returns them). */
+ * [coils][n] (t = coil images of M p, tb = those of M qb, as tsn_normal returns them).
+ * qb_norm_parts (optional, TSN_CG_STEP_PARTS device doubles) receives partial sums of |qb|^2
+ * for the tsn_normal of qb. */
 tsn_status tsn_cg_adjoint_step(tsn_plan* plan, int64_t n, const double* rho, const double* rho_next,
                                const double* gamma, const double* rhob, double* rhob_out, void* rb,
                                void* pb, const void* p, const void* q, const void* r_next,
-                               const void* xb, void* qb, tsn_stream_t stream);
+                               const void* xb, void* qb, double* qb_norm_parts,
+                               tsn_stream_t stream);
 tsn_status tsn_cg_adjoint_finish(tsn_plan* plan, int64_t n, int32_t coils, void* pb, const void* mqb,
                                  const void* qb, const void* coil_images, const void* coil_images_bar,
                                  const void* p, void* sb, tsn_stream_t stream);

@@ -23,6 +23,7 @@ ILLEGAL = {"split24": 0, "csr_residual": 1}
 VIEW = {"G": 0, "G_T": 1}
 FLAG_REFERENCE_LAYOUT = 1
 FLAG_REFERENCE_STEPS = 2
+CG_STEP_PARTS = 296  # TSN_CG_STEP_PARTS
 STAGES = ("fwd_rows", "fwd_cols", "interp_fwd", "interp_adj", "inv_cols", "inv_rows", "cg_update", "fwd_mid",
           "inv_mid")
 
@@ -113,10 +114,10 @@ def lib() -> C.CDLL:
         "tsn_forward": (C.c_int, [P, P, P, P, P]),
         "tsn_adjoint": (C.c_int, [P, P, P, P, P]),
         "tsn_forward_reference": (C.c_int, [P, P, P, P, P]),
-        "tsn_normal": (C.c_int, [P, P, P, P, C.c_float, P, P, P, P]),
+        "tsn_normal": (C.c_int, [P, P, P, P, C.c_float, P, P, P, P, C.c_int32, P]),
         "tsn_rdot": (C.c_int, [P, P, P, C.c_int64, P, P]),
-        "tsn_cg_step": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P]),
-        "tsn_cg_adjoint_step": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P]),
+        "tsn_cg_step": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P]),
+        "tsn_cg_adjoint_step": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
         "tsn_cg_adjoint_finish": (C.c_int, [P, C.c_int64, C.c_int32, P, P, P, P, P, P, P, P]),
         "tsn_adjoint_reference": (C.c_int, [P, P, P, P, P]),
         "tsn_cg_sense": (C.c_int, [P, P, P, P, F32, F32, I32, P, PF64, C.POINTER(CgStatus), P]),

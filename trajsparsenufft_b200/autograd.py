@@ -42,11 +42,13 @@ class PlanOps:
     def adjoint_coils(self, y: torch.Tensor) -> torch.Tensor:
         return self.plan.adjoint(y.contiguous())
 
-    def normal(self, p, smaps, density, lam, coils=False, pq=False):
+    def normal(self, p, smaps, density, lam, coils=False, pq=False, p_parts=None):
         """(sum_c conj(S_c) G(S_c p) + lam p, the coil images G(S_c p) or None, Re <p, q> or
         None) in the plan's kernels (tsn_normal): SENSE expansion, weighting, combine and the
-        FP64 inner product fused into the NUFFT stages."""
-        return self.plan.normal(p.contiguous(), smaps.contiguous(), density=density, lam=lam, coils=coils, pq=pq)
+        FP64 inner product fused into the NUFFT stages. p_parts: FP64 partials of |p|^2 from
+        the CG step that made p."""
+        return self.plan.normal(p.contiguous(), smaps.contiguous(), density=density, lam=lam, coils=coils, pq=pq,
+                                p_norm_parts=p_parts)
 
     def rdot(self, a, b):
         """Re <a, b> in FP64, fixed order (tsn_rdot), as a 0-d device tensor."""
@@ -57,13 +59,14 @@ class PlanOps:
         return self.plan.forward(x.contiguous(), smaps.contiguous())
 
     def step(self, rho, gamma, x, p, r, q):
-        """One CG step in the plan's kernels: (x' or None, r', p', rho')."""
+        """One CG step in the plan's kernels: (x' or None, r', p', rho', |p'|^2 partials)."""
         return self.plan.cg_step(rho, gamma, None if x is None else x.contiguous(), p.contiguous(), r.contiguous(),
-                                 q.contiguous())
+                                 q.contiguous(), norm_parts=True)
 
     def adjoint_step(self, rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb):
-        """Reverse-mode CG step in the plan's kernels (rb, pb in place): (qb, rhob of the step)."""
-        return self.plan.cg_adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb)
+        """Reverse-mode CG step in the plan's kernels (rb, pb in place): (qb, rhob of the step,
+        |qb|^2 partials)."""
+        return self.plan.cg_adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb, norm_parts=True)
 
     def adjoint_finish(self, pb, mqb, qb=None, t=None, tb=None, p=None, sb=None):
         """pb += M qb and the coil-map cotangent update, in place."""
@@ -104,41 +107,43 @@ class _Sense:
         """F(S x), the coil k-space of image x."""
         return self.ops.forward_maps(x, self.s) if self.fused else self.ops.forward_coils(self.s * x)
 
-    def M(self, p):
+    # `parts` below: FP64 partial sums of |p|^2 that the fused CG steps hand to the next
+    # normal-operator application (its panel scale); None computes them there.
+    def M(self, p, parts=None):
         if self.fused:
-            return self.ops.normal(p, self.s, self.w, self.lam)[0]
+            return self.ops.normal(p, self.s, self.w, self.lam, p_parts=parts)[0]
         return self.combine(self.G(self.s * p)) + self.lam * p
 
-    def M_dot(self, p):
+    def M_dot(self, p, parts=None):
         """(M p, Re <p, M p>)."""
         if self.fused:
-            q, _, pq = self.ops.normal(p, self.s, self.w, self.lam, pq=True)
+            q, _, pq = self.ops.normal(p, self.s, self.w, self.lam, pq=True, p_parts=parts)
             return q, pq
         q = self.M(p)
         return q, _rdot(p, q)
 
-    def M_coils_dot(self, p):
+    def M_coils_dot(self, p, parts=None):
         """(M p, the coil images G(S p), Re <p, M p>)."""
         if self.fused:
-            return self.ops.normal(p, self.s, self.w, self.lam, coils=True, pq=True)
+            return self.ops.normal(p, self.s, self.w, self.lam, coils=True, pq=True, p_parts=parts)
         q, t = self.M_coils(p)
         return q, t, _rdot(p, q)
 
     def step(self, rho, gamma, x, p, r, q):
-        """CG step: (x + alpha p or None, r' = r - alpha q, p' = r' + (rho'/rho) p, rho' = |r'|^2)
-        with alpha = rho / gamma."""
+        """CG step: (x + alpha p or None, r' = r - alpha q, p' = r' + (rho'/rho) p, rho' = |r'|^2,
+        the |p'|^2 partials or None) with alpha = rho / gamma."""
         if self.fused:
             return self.ops.step(rho, gamma, x, p, r, q)
         alpha = rho / gamma
         x_n = None if x is None else x + alpha * p
         r_n = r - alpha * q
         rho_n = _rdot(r_n, r_n)
-        return x_n, r_n, r_n + (rho_n / rho) * p, rho_n
+        return x_n, r_n, r_n + (rho_n / rho) * p, rho_n, None
 
-    def M_coils(self, p):
+    def M_coils(self, p, parts=None):
         """(M p, the coil images G(S p)) — the second feeds the coil-map gradient."""
         if self.fused:
-            q, t, _ = self.ops.normal(p, self.s, self.w, self.lam, coils=True)
+            q, t, _ = self.ops.normal(p, self.s, self.w, self.lam, coils=True, p_parts=parts)
             return q, t
         t = self.G(self.s * p)
         return self.combine(t) + self.lam * p, t
@@ -205,15 +210,16 @@ class UnrolledCgSense(torch.autograd.Function):
         cps = [(x, r, p, rho)]
         need_s = ctx.needs_input_grad[1]
         firsts = []   # q = M p (and the coil images G(S p) when maps need gradients) of each
+        parts = None
         for k in range(iters):   # checkpointed step: the backward reuses them instead of recomputing
             if k % checkpoint == 0 and need_s:
-                q, t, gamma = S.M_coils_dot(p)
+                q, t, gamma = S.M_coils_dot(p, parts)
                 firsts.append((q, t))
             else:
-                q, gamma = S.M_dot(p)
+                q, gamma = S.M_dot(p, parts)
                 if k % checkpoint == 0:
                     firsts.append((q,))
-            x, r, p, rho = S.step(rho, gamma, x, p, r, q)
+            x, r, p, rho, parts = S.step(rho, gamma, x, p, r, q)
             if (k + 1) % checkpoint == 0 and k + 1 < iters:
                 cps.append((x, r, p, rho))
         ctx.ops, ctx.lam, ctx.iters, ctx.checkpoint, ctx.x0_zero = ops, lam, iters, checkpoint, x0_zero
@@ -246,27 +252,28 @@ class UnrolledCgSense(torch.autograd.Function):
             k0, k1 = seg * c, min(seg * c + c, iters)
             _, r, p, rho = cps[seg]
             steps = []
+            parts = None
             for k in range(k0, k1):  # recompute this segment's forward states
                 if k == k0:          # kept by the forward with the checkpoint
                     q, t = firsts[seg][0], (firsts[seg][1] if need_s else None)
                 elif need_s:
-                    q, t = S.M_coils(p)
+                    q, t = S.M_coils(p, parts)
                 else:
-                    q, t = S.M(p), None
+                    q, t = S.M(p, parts), None
                 gamma = S.dot(p, q)
-                _, r_n, p_n, rho_n = S.step(rho, gamma, None, p, r, q)
+                _, r_n, p_n, rho_n, parts = S.step(rho, gamma, None, p, r, q)
                 ab = (None, None) if S.fused else (rho / gamma, rho_n / rho)  # alpha, beta: composed path
                 steps.append((p, q, t, r_n, rho, rho_n, gamma, *ab))
                 p = p_n
                 r, rho = r_n, rho_n
             for p, q, t, r_n, rho, rho_n, gamma, alpha, beta in reversed(steps):
                 if S.fused:  # the same recurrences in the plan's kernels (rb, pb, sb in place)
-                    qb, rhob = ctx.ops.adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb)
+                    qb, rhob, qparts = ctx.ops.adjoint_step(rho, rho_n, gamma, rhob, rb, pb, p, q, r_n, xb)
                     if need_s:
-                        mqb, tb = S.M_coils(qb)
+                        mqb, tb = S.M_coils(qb, qparts)
                         ctx.ops.adjoint_finish(pb, mqb, qb, t, tb, p, sb)
                     else:
-                        ctx.ops.adjoint_finish(pb, S.M(qb))
+                        ctx.ops.adjoint_finish(pb, S.M(qb, qparts))
                     continue
                 rb = rb + pb                                   # p' = r' + beta p
                 betab = S.dot(pb, p)

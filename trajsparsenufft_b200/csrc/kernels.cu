@@ -1475,7 +1475,7 @@ void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_
 //   rhobk = -<pb, p> rho' / rho^2 + alphab / gamma
 // with <rb2, q> = <rb, q> + <pb, q> + 2 rhob_n <r', q>, so the five FP64 inner products come
 // from one pass over the vectors before any of them changes.
-constexpr int kCgbBlocks = 296;  // 2 x 148 SMs
+constexpr int kCgbBlocks = kCgStepParts;  // 2 x 148 SMs
 
 __global__ void cgb_dots_kernel(int64_t n, const float2* __restrict__ rb, const float2* __restrict__ pb,
                                 const float2* __restrict__ p, const float2* __restrict__ q,
@@ -1514,7 +1514,7 @@ __global__ void cgb_update_kernel(int64_t n, int nparts, const double* __restric
                                   double* __restrict__ rhob_out, float2* __restrict__ rb, float2* __restrict__ pb,
                                   const float2* __restrict__ p, const float2* __restrict__ q,
                                   const float2* __restrict__ rn, const float2* __restrict__ xb,
-                                  float2* __restrict__ qb) {
+                                  float2* __restrict__ qb, double* __restrict__ qnorm_parts) {
   __shared__ double red[132];
   __shared__ double dl[5];
   const double4 s4 = sum_partials4(parts, nparts, nparts, red);
@@ -1536,13 +1536,20 @@ __global__ void cgb_update_kernel(int64_t n, int nparts, const double* __restric
   if (blockIdx.x == 0 && threadIdx.x == 0) *rhob_out = -betab * rho_n / (rho * rho) + alphab / gamma;
   const float a = static_cast<float>(alpha), b = static_cast<float>(beta), g = static_cast<float>(gammab),
               h = static_cast<float>(2.0 * rhob_n);
+  double acc = 0.0;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const float2 vrb = rb[i], vpb = pb[i], vp = p[i], vq = q[i], vrn = rn[i], vxb = xb[i];
     const float2 r2 = make_float2(vrb.x + vpb.x + h * vrn.x, vrb.y + vpb.y + h * vrn.y);
     rb[i] = r2;
-    qb[i] = make_float2(-a * r2.x + g * vp.x, -a * r2.y + g * vp.y);
+    const float2 qv = make_float2(-a * r2.x + g * vp.x, -a * r2.y + g * vp.y);
+    qb[i] = qv;
+    acc += static_cast<double>(qv.x) * qv.x + static_cast<double>(qv.y) * qv.y;
     pb[i] = make_float2(b * vpb.x + a * vxb.x + g * vq.x, b * vpb.y + a * vxb.y + g * vq.y);
+  }
+  if (qnorm_parts) {  // |qb|^2 partials: the panel scale of the M qb that follows
+    const double t = block_sum(acc, red);
+    if (threadIdx.x == 0) qnorm_parts[blockIdx.x] = t;
   }
 }
 
@@ -1597,34 +1604,44 @@ __global__ void cgf_update_kernel(int64_t n, const double* __restrict__ rho_p, c
   if (threadIdx.x == 0) parts[blockIdx.x] = t;
 }
 
+// With pnorm_parts given, also one FP64 partial of |p'|^2 per block (the panel scale of the
+// next normal-operator application, which then needs no norm pass of its own).
 __global__ void cgf_direction_kernel(int64_t n, int nparts, const double* __restrict__ parts,
                                      const double* __restrict__ rho_p, double* __restrict__ rho_out,
                                      const float2* __restrict__ p, const float2* __restrict__ r_new,
-                                     float2* __restrict__ p_out) {
+                                     float2* __restrict__ p_out, double* __restrict__ pnorm_parts) {
   __shared__ double red[33];
   const double rho_n = sum_partials(parts, nparts, red);
   if (blockIdx.x == 0 && threadIdx.x == 0) *rho_out = rho_n;
   const float b = static_cast<float>(rho_n / *rho_p);
+  double acc = 0.0;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const float2 vp = p[i], vr = r_new[i];
-    p_out[i] = make_float2(vr.x + b * vp.x, vr.y + b * vp.y);
+    const float2 pn = make_float2(vr.x + b * vp.x, vr.y + b * vp.y);
+    p_out[i] = pn;
+    acc += static_cast<double>(pn.x) * pn.x + static_cast<double>(pn.y) * pn.y;
+  }
+  if (pnorm_parts) {
+    const double t = block_sum(acc, red);
+    if (threadIdx.x == 0) pnorm_parts[blockIdx.x] = t;
   }
 }
 
 void launch_cg_step(int64_t n, double* parts, const double* rho, const double* gamma, const float2* x, const float2* p,
                     const float2* r, const float2* q, float2* x_out, float2* r_out, float2* p_out, double* rho_out,
-                    cudaStream_t s) {
+                    double* p_norm_parts, cudaStream_t s) {
   cgf_update_kernel<<<kCgbBlocks, 256, 0, s>>>(n, rho, gamma, x, p, r, q, x_out, r_out, parts);
-  cgf_direction_kernel<<<kCgbBlocks, 256, 0, s>>>(n, kCgbBlocks, parts, rho, rho_out, p, r_out, p_out);
+  cgf_direction_kernel<<<kCgbBlocks, 256, 0, s>>>(n, kCgbBlocks, parts, rho, rho_out, p, r_out, p_out, p_norm_parts);
 }
 
 void launch_cg_adjoint_step(int64_t n, double* parts, const double* rho, const double* rho_n, const double* gamma,
                             const double* rhob, double* rhob_out, float2* rb, float2* pb, const float2* p,
-                            const float2* q, const float2* rn, const float2* xb, float2* qb, cudaStream_t s) {
+                            const float2* q, const float2* rn, const float2* xb, float2* qb, double* qb_norm_parts,
+                            cudaStream_t s) {
   cgb_dots_kernel<<<kCgbBlocks, 256, 0, s>>>(n, rb, pb, p, q, rn, xb, parts);
   cgb_update_kernel<<<kCgbBlocks, 256, 0, s>>>(n, kCgbBlocks, parts, rho, rho_n, gamma, rhob, rhob_out, rb, pb, p, q,
-                                                rn, xb, qb);
+                                                rn, xb, qb, qb_norm_parts);
 }
 
 void launch_cg_adjoint_finish(int64_t n, int coils, float2* pb, const float2* mqb, const float2* qb, const float2* t,

@@ -221,12 +221,14 @@ void launch_sum_partials_to(const double* parts, int n, double* out, cudaStream_
 // p_out = r_out + (rho_out / rho) p.
 void launch_cg_step(int64_t n, double* parts, const double* rho, const double* gamma, const float2* x, const float2* p,
                     const float2* r, const float2* q, float2* x_out, float2* r_out, float2* p_out, double* rho_out,
-                    cudaStream_t s);
+                    double* p_norm_parts, cudaStream_t s);
+constexpr int kCgStepParts = 296;  // FP64 partials of the CG-step kernels (one per block)
 // Reverse-mode CG step (kernels.cu): five FP64 inner products in one pass (parts: 5 x 296
 // doubles), then rb, pb updated in place, qb written and rhob of the step to *rhob_out.
 void launch_cg_adjoint_step(int64_t n, double* parts, const double* rho, const double* rho_n, const double* gamma,
                             const double* rhob, double* rhob_out, float2* rb, float2* pb, const float2* p,
-                            const float2* q, const float2* rn, const float2* xb, float2* qb, cudaStream_t s);
+                            const float2* q, const float2* rn, const float2* xb, float2* qb, double* qb_norm_parts,
+                            cudaStream_t s);
 // pb += mqb and, with sb given, the coil-map cotangent sb[c] += conj(qb) t[c] + tb[c] conj(p).
 void launch_cg_adjoint_finish(int64_t n, int coils, float2* pb, const float2* mqb, const float2* qb, const float2* t,
                               const float2* tb, const float2* p, float2* sb, cudaStream_t s);

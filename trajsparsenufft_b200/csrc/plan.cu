@@ -1060,13 +1060,19 @@ void enqueue_forward(tsn_plan* P, const void* x, const void* smaps, void* y, cud
 // scale 1), with the optional coil images A_c^H W A p before the coil combine and the optional
 // FP64 Re <p, q>: the plain forward's panel scale, both interpolations, the inverse FFTs and
 // the combine epilogue (inv_rows mode 5).
+static_assert(kCgStepParts == TSN_CG_STEP_PARTS, "CG-step partial count of the kernels and the header");
+
 void enqueue_normal(tsn_plan* P, const void* p, const void* smaps, const float* density, float lambda, void* q,
-                    void* coils, double* pq, cudaStream_t s) {
+                    void* coils, double* pq, const double* p_parts, int n_p_parts, cudaStream_t s) {
   const FftArgs f = fft_args(P, smaps);
   CgState* st = P->state.as<CgState>();
   const float2* pv = static_cast<const float2*>(p);
-  launch_norm_partials(pv, image_pixels(P), P->norm_parts.as<double>(), s);
-  fwd_chain(P, f, pv, 0, nullptr, nullptr, P->norm_parts.as<double>(), kNormParts, st, 0, P->panel.as<__half>(), s);
+  if (!p_parts) {  // the panel scale of p from |p|^2 partials, unless the caller has them
+    launch_norm_partials(pv, image_pixels(P), P->norm_parts.as<double>(), s);
+    p_parts = P->norm_parts.as<double>();
+    n_p_parts = kNormParts;
+  }
+  fwd_chain(P, f, pv, 0, nullptr, nullptr, p_parts, n_p_parts, st, 0, P->panel.as<__half>(), s);
   InterpOut of;
   of.panel = P->spanel.as<__half>();
   of.density = density;
@@ -1274,13 +1280,16 @@ tsn_status tsn_adjoint(tsn_plan* plan, const void* y, const void* smaps, void* x
 }
 
 tsn_status tsn_normal(tsn_plan* plan, const void* p, const void* smaps, const float* density, float lambda, void* q,
-                      void* coil_images, double* pq, tsn_stream_t stream) {
+                      void* coil_images, double* pq, const double* p_norm_parts, int32_t n_p_norm_parts,
+                      tsn_stream_t stream) {
   try {
     if (!plan || !p || !smaps || !q) fail(TSN_ERR_ARG, "NULL argument (p, smaps and q are required)");
     if (!std::isfinite(lambda)) fail(TSN_ERR_ARG, "lambda must be finite");
+    if (p_norm_parts && n_p_norm_parts <= 0) fail(TSN_ERR_ARG, "n_p_norm_parts must be positive");
     need_aligned({p, smaps, q, coil_images, density});
     need_views(plan, true, true);
-    enqueue_normal(plan, p, smaps, density, lambda, q, coil_images, pq, reinterpret_cast<cudaStream_t>(stream));
+    enqueue_normal(plan, p, smaps, density, lambda, q, coil_images, pq, p_norm_parts, n_p_norm_parts,
+                   reinterpret_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
     return TSN_OK;
   } catch (const std::exception& e) {
@@ -1304,7 +1313,7 @@ tsn_status tsn_rdot(tsn_plan* plan, const void* a, const void* b, int64_t n, dou
 
 tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const double* gamma, const void* x, const void* p,
                        const void* r, const void* q, void* x_out, void* r_out, void* p_out, double* rho_out,
-                       tsn_stream_t stream) {
+                       double* p_norm_parts, tsn_stream_t stream) {
   try {
     if (!plan || !rho || !gamma || !p || !r || !q || !r_out || !p_out || !rho_out) fail(TSN_ERR_ARG, "NULL argument");
     if ((x == nullptr) != (x_out == nullptr)) fail(TSN_ERR_ARG, "x and x_out go together");
@@ -1313,7 +1322,7 @@ tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const doubl
     launch_cg_step(n, plan->adj_parts.as<double>(), rho, gamma, static_cast<const float2*>(x),
                    static_cast<const float2*>(p), static_cast<const float2*>(r), static_cast<const float2*>(q),
                    static_cast<float2*>(x_out), static_cast<float2*>(r_out), static_cast<float2*>(p_out), rho_out,
-                   reinterpret_cast<cudaStream_t>(stream));
+                   p_norm_parts, reinterpret_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
     return TSN_OK;
   } catch (const std::exception& e) {
@@ -1324,7 +1333,7 @@ tsn_status tsn_cg_step(tsn_plan* plan, int64_t n, const double* rho, const doubl
 tsn_status tsn_cg_adjoint_step(tsn_plan* plan, int64_t n, const double* rho, const double* rho_next,
                                const double* gamma, const double* rhob, double* rhob_out, void* rb, void* pb,
                                const void* p, const void* q, const void* r_next, const void* xb, void* qb,
-                               tsn_stream_t stream) {
+                               double* qb_norm_parts, tsn_stream_t stream) {
   try {
     if (!plan || !rho || !rho_next || !gamma || !rhob || !rhob_out || !rb || !pb || !p || !q || !r_next || !xb || !qb)
       fail(TSN_ERR_ARG, "NULL argument");
@@ -1333,7 +1342,7 @@ tsn_status tsn_cg_adjoint_step(tsn_plan* plan, int64_t n, const double* rho, con
     launch_cg_adjoint_step(n, plan->adj_parts.as<double>(), rho, rho_next, gamma, rhob, rhob_out,
                            static_cast<float2*>(rb), static_cast<float2*>(pb), static_cast<const float2*>(p),
                            static_cast<const float2*>(q), static_cast<const float2*>(r_next),
-                           static_cast<const float2*>(xb), static_cast<float2*>(qb),
+                           static_cast<const float2*>(xb), static_cast<float2*>(qb), qb_norm_parts,
                            reinterpret_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
     return TSN_OK;

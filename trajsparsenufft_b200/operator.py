@@ -189,10 +189,13 @@ class Plan:
         check(fn(self._h, yp, sp, xp, _stream_handle(stream)))
         return out
 
-    def normal(self, p, smaps, *, density=None, lam=0.0, out=None, coils=False, pq=False, stream=None):
+    def normal(self, p, smaps, *, density=None, lam=0.0, out=None, coils=False, pq=False, p_norm_parts=None,
+               stream=None):
         """q = A^H W A p + lam p (tsn_normal): the CG's normal operator on image p [N, N] with
         coil maps.  coils=True also returns the coil images A_c^H W A p [C, N, N] before the
         combine; pq=True also returns Re <p, q> as a 0-d FP64 tensor on the device (no sync).
+        p_norm_parts: an FP64 device tensor whose sum is |p|^2 (as cg_step returns for its p'),
+        which saves the pass that computes it.
         Returns (q, coil images or None, Re <p, q> or None)."""
         torch = _torch()
         cf = torch.complex64
@@ -205,7 +208,13 @@ class Plan:
         t = torch.empty(self.maps_shape, dtype=cf, device=p.device) if coils else None
         tp = None if t is None else _dev_ptr(t, cf, self.maps_shape, "coils")
         d = torch.empty((), dtype=torch.float64, device=p.device) if pq else None
-        check(lib().tsn_normal(self._h, pp, sp, dp, float(lam), qp, tp, None if d is None else d.data_ptr(),
+        if p_norm_parts is not None:
+            if p_norm_parts.dtype != torch.float64 or not p_norm_parts.is_cuda or not p_norm_parts.is_contiguous():
+                raise TypeError("p_norm_parts must be a contiguous float64 CUDA tensor")
+            npp, npn = C.c_void_p(p_norm_parts.data_ptr()), int(p_norm_parts.numel())
+        else:
+            npp, npn = None, 0
+        check(lib().tsn_normal(self._h, pp, sp, dp, float(lam), qp, tp, None if d is None else d.data_ptr(), npp, npn,
                                _stream_handle(stream)))
         return out, t, d
 
@@ -221,9 +230,10 @@ class Plan:
         check(lib().tsn_rdot(self._h, ap, bp, int(a.numel()), d.data_ptr(), _stream_handle(stream)))
         return d
 
-    def cg_step(self, rho, gamma, x, p, r, q, stream=None):
+    def cg_step(self, rho, gamma, x, p, r, q, norm_parts=False, stream=None):
         """One CG step on image vectors (tsn_cg_step): returns (x' or None, r', p', rho' as a
-        0-d FP64 device tensor) with alpha = rho / gamma; x may be None."""
+        0-d FP64 device tensor, and with norm_parts=True the FP64 partials of |p'|^2 for the
+        next normal()) with alpha = rho / gamma; x may be None."""
         torch = _torch()
         shape = tuple(p.shape)
         cf = torch.complex64
@@ -231,15 +241,18 @@ class Plan:
         xo = None if x is None else torch.empty(shape, dtype=cf, device=p.device)
         ro, po = torch.empty(shape, dtype=cf, device=p.device), torch.empty(shape, dtype=cf, device=p.device)
         rho_o = torch.empty((), dtype=torch.float64, device=p.device)
+        parts = torch.empty(_lib.CG_STEP_PARTS, dtype=torch.float64, device=p.device) if norm_parts else None
         check(lib().tsn_cg_step(self._h, int(p.numel()), *sc, None if x is None else _dev_ptr(x, cf, shape, "x"),
                                 _dev_ptr(p, cf, shape, "p"), _dev_ptr(r, cf, shape, "r"), _dev_ptr(q, cf, shape, "q"),
                                 None if xo is None else C.c_void_p(xo.data_ptr()), C.c_void_p(ro.data_ptr()),
-                                C.c_void_p(po.data_ptr()), C.c_void_p(rho_o.data_ptr()), _stream_handle(stream)))
-        return xo, ro, po, rho_o
+                                C.c_void_p(po.data_ptr()), C.c_void_p(rho_o.data_ptr()),
+                                None if parts is None else C.c_void_p(parts.data_ptr()), _stream_handle(stream)))
+        return (xo, ro, po, rho_o, parts) if norm_parts else (xo, ro, po, rho_o)
 
-    def cg_adjoint_step(self, rho, rho_next, gamma, rhob, rb, pb, p, q, r_next, xb, stream=None):
+    def cg_adjoint_step(self, rho, rho_next, gamma, rhob, rb, pb, p, q, r_next, xb, norm_parts=False, stream=None):
         """One reverse-mode CG step (tsn_cg_adjoint_step): rb and pb (complex64, one image each)
-        are updated in place; returns (qb, the cotangent of rho as a 0-d FP64 device tensor).
+        are updated in place; returns (qb, the cotangent of rho as a 0-d FP64 device tensor, and
+        with norm_parts=True the FP64 partials of |qb|^2 for normal(qb)).
         rho, rho_next, gamma, rhob are 0-d FP64 device tensors."""
         torch = _torch()
         shape = tuple(p.shape)
@@ -249,9 +262,11 @@ class Plan:
                ((rb, "rb"), (pb, "pb"), (p, "p"), (q, "q"), (r_next, "r_next"), (xb, "xb"))]
         qb = torch.empty(shape, dtype=torch.complex64, device=p.device)
         rhob_out = torch.empty((), dtype=torch.float64, device=p.device)
+        parts = torch.empty(_lib.CG_STEP_PARTS, dtype=torch.float64, device=p.device) if norm_parts else None
         check(lib().tsn_cg_adjoint_step(self._h, int(p.numel()), *ptrs, C.c_void_p(rhob_out.data_ptr()), *vec,
-                                        C.c_void_p(qb.data_ptr()), _stream_handle(stream)))
-        return qb, rhob_out
+                                        C.c_void_p(qb.data_ptr()), None if parts is None else C.c_void_p(parts.data_ptr()),
+                                        _stream_handle(stream)))
+        return (qb, rhob_out, parts) if norm_parts else (qb, rhob_out)
 
     def cg_adjoint_finish(self, pb, mqb, qb=None, t=None, tb=None, p=None, sb=None, stream=None):
         """pb += mqb in place and, with sb given, sb[c] += conj(qb) t[c] + tb[c] conj(p)
