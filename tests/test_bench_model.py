@@ -39,3 +39,16 @@ def test_volume_bytes_share_the_solve_model():
     rhs = ("interp_adj", "inv_cols", "inv_mid", "inv_rows")
     per_iter = sum(v for k, v in alg.items() if k != "cg_update")
     assert bench.solve_bytes(alg, 10, img, rhs) == 10 * per_iter - 6 * img + alg["cg_update"] + sum(alg[k] for k in rhs)
+
+
+def test_numa_local_is_a_no_op_without_nvml_answer():
+    """bench.NumaLocal pins the allocating thread to the GPU's NUMA-local CPUs only when NVML
+    names them; without a GPU it changes nothing and says so."""
+    import os
+    before = os.sched_getaffinity(0)
+    with bench.NumaLocal(0) as numa:
+        assert os.sched_getaffinity(0) == (numa.cpus or before)
+    assert os.sched_getaffinity(0) == before
+    info = numa.summary()
+    assert info["allowed_cpus"] == len(before)
+    assert info["pinned_on_gpu_node"] == bool(numa.cpus)
